@@ -1,0 +1,229 @@
+"""cuopo3d_b200 -- B200-native split-step Fourier solver for three coupled chi(2)
+fields (pump, signal, idler) in an optical parametric oscillator.
+
+The compute path is the in-tree CUDA library ``libcuopo3d.so`` (sm_100a kernels and
+the C-ABI of include/cuopo3d.h).  This module binds that C-ABI with ctypes and mirrors
+the reference's classes (alfredos84/cuOPO3D src/headers: crystals, Cavity, EFields,
+Solver) so that scripts written against the reference read the same.  There is no
+CPU fallback: importing works without a GPU, but creating a solver without the
+library or without a CUDA device raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcuopo3d.so")
+
+# status codes
+OPO_OK, OPO_ERR_INVALID, OPO_ERR_CUDA, OPO_ERR_NOMEM, OPO_ERR_NONFINITE = 0, 1, 2, 3, 4
+OPO_ERR_COURANT, OPO_ERR_CAPACITY = 5, 6
+# flags
+DISPERSION, DIFFRACTION, PHYSICS, ASIS_Q1, ASIS_Q2 = 1, 2, 4, 8, 16
+FP32, FP64 = 0, 1
+PPLN_ID, MGOSPPLT_ID = 0, 1
+FIELD_API, FIELD_AP, FIELD_AS, FIELD_AI = 0, 1, 2, 3
+MEM_HOST, MEM_DEVICE = 0, 1
+PUMP_MODES = {"waveplane-cw": 0, "waveplane-pulsed": 1, "focused-cw": 2, "focused-pulsed": 3,
+              "focused-sech2": 4, "waveplane-sech2": 5}
+SCALAR_NAMES = ("np ns ni vp vs vi b2p b2s b2i b3p b3s b3i dQ dk dx dy dz kp ks ki "
+                "kappa_p kappa_s kappa_i trt dt nsteps").split()
+
+_d = ctypes.c_double
+_i = ctypes.c_int
+_u = ctypes.c_uint
+
+
+class OpoConfig(ctypes.Structure):
+    _fields_ = [("crystal", _i), ("LX", _d), ("LY", _d), ("Lcr", _d), ("T", _d), ("Lambda", _d),
+                ("lp", _d), ("ls", _d), ("nx", _i), ("ny", _i), ("nt", _i), ("nz", _i), ("dQ", _d),
+                ("alpha", _d * 3), ("Lcav", _d), ("Rs", _d), ("Ri", _d), ("gdd_gamma", _d),
+                ("detuning", _d), ("P", _d), ("FWHM", _d), ("w0", _d), ("focal", _d),
+                ("pump_mode", _i), ("t_window", _d), ("flags", _u), ("zloop_f32", _i),
+                ("n_steps", _i), ("total_rt", _i), ("precision", _i), ("resonant", _u)]
+
+
+class OpoParams(ctypes.Structure):
+    _fields_ = [("nx", _i), ("ny", _i), ("nt", _i), ("n_steps", _i), ("flags", _u),
+                ("precision", _i), ("dz", _d), ("Lcr", _d), ("dx", _d), ("dy", _d),
+                ("kappa", _d * 3), ("kdiff", _d * 3), ("vinv", _d * 3), ("beta2", _d * 3),
+                ("alpha", _d * 3), ("dk", _d), ("Rs", _d), ("Ri", _d), ("detuning", _d),
+                ("gdd", _d), ("free_len", _d), ("resonant", _u), ("total_rt", _i),
+                ("t_window", _d)]
+
+
+class OpoError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cuopo3d error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libcuopo3d.so (built in-tree by cuopo3d_b200.build); raises if absent."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing: build it with `python -m cuopo3d_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.opo_params_from_config.argtypes = [ctypes.POINTER(OpoConfig), ctypes.POINTER(OpoParams), dp]
+        L.opo_crystal_dispersion.argtypes = [_i, _d, _d, dp]
+        L.opo_time_freq.argtypes = [_i, _d, dp, dp]
+        L.opo_pump_field.argtypes = [ctypes.POINTER(OpoConfig), dp]
+        L.opo_noise.argtypes = [ctypes.c_uint64, _d, ctypes.c_size_t, dp]
+        L.opo_create.argtypes = [ctypes.POINTER(OpoParams), dp, ctypes.POINTER(vp)]
+        L.opo_destroy.argtypes = [vp]
+        L.opo_destroy.restype = None
+        L.opo_set_field.argtypes = [vp, _i, vp, _i, _i]
+        L.opo_get_field.argtypes = [vp, _i, vp, _i, _i]
+        L.opo_run_single_pass.argtypes = [vp]
+        L.opo_run_round_trips.argtypes = [vp, _i]
+        L.opo_field_sums.argtypes = [vp, dp]
+        L.opo_synchronize.argtypes = [vp]
+        L.opo_round_trip_index.argtypes = [vp]
+        L.opo_kernel_launches.argtypes = [vp]
+        L.opo_kernel_launches.restype = ctypes.c_longlong
+        L.opo_last_error.argtypes = [vp]
+        L.opo_last_error.restype = ctypes.c_char_p
+        L.opo_version.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def _dptr(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def make_config(**kw):
+    """OpoConfig with the reference main()'s defaults (cuOPO3D.cu:15-46) overridden by kw."""
+    d = dict(crystal=PPLN_ID, LX=400.0, LY=400.0, Lcr=5000.0, T=27.0, Lambda=6.97, lp=0.532,
+             ls=1.064, nx=16, ny=16, nt=32, nz=10, dQ=-1.0, alpha=(-1.0, -1.0, -1.0), Lcav=-1.0,
+             Rs=0.98, Ri=None, gdd_gamma=0.0, detuning=0.0, P=1.0, FWHM=2.0, w0=50.0, focal=None,
+             pump_mode="focused-pulsed", t_window=0.0, flags=DISPERSION | DIFFRACTION,
+             zloop_f32=0, n_steps=0, total_rt=1, precision=FP64, resonant=6)
+    d.update(kw)
+    if d["Ri"] is None:
+        d["Ri"] = d["Rs"]
+    if d["focal"] is None:
+        d["focal"] = d["Lcr"] / 2
+    if isinstance(d["pump_mode"], str):
+        d["pump_mode"] = PUMP_MODES[d["pump_mode"]]
+    if isinstance(d["crystal"], str):
+        d["crystal"] = {"ppln": PPLN_ID, "mgosplt": MGOSPPLT_ID, "mgosppl t": MGOSPPLT_ID}[d["crystal"].lower()]
+    c = OpoConfig()
+    for k, v in d.items():
+        if k == "alpha":
+            c.alpha = (_d * 3)(*v)
+        else:
+            setattr(c, k, v)
+    return c
+
+
+def derive(cfg):
+    """(OpoParams, scalars dict) of a config (the reference constructors)."""
+    p = OpoParams()
+    sc = np.zeros(len(SCALAR_NAMES))
+    rc = lib().opo_params_from_config(ctypes.byref(cfg), ctypes.byref(p), _dptr(sc))
+    if rc:
+        raise OpoError(rc, "opo_params_from_config rejected the configuration")
+    return p, dict(zip(SCALAR_NAMES, sc))
+
+
+def time_freq(nt, window):
+    t, w = np.zeros(nt), np.zeros(nt)
+    rc = lib().opo_time_freq(nt, window, _dptr(t), _dptr(w))
+    if rc:
+        raise OpoError(rc, "opo_time_freq")
+    return t, w
+
+
+def pump_field(cfg):
+    a = np.zeros(2 * cfg.nx * cfg.ny * cfg.nt)
+    rc = lib().opo_pump_field(ctypes.byref(cfg), _dptr(a))
+    if rc:
+        raise OpoError(rc, "opo_pump_field")
+    return a.view(np.complex128).reshape(cfg.nt, cfg.ny, cfg.nx)
+
+
+def noise(seed, sigma, n):
+    a = np.zeros(2 * n)
+    lib().opo_noise(seed, sigma, n, _dptr(a))
+    return a.view(np.complex128)
+
+
+class Simulation:
+    """One resident solver (fields, tables, plans) on the current CUDA device."""
+
+    def __init__(self, params, w):
+        self.params = params
+        self.shape = (params.nt, params.ny, params.nx)
+        self._h = ctypes.c_void_p()
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        rc = lib().opo_create(ctypes.byref(params), _dptr(w), ctypes.byref(self._h))
+        if rc:
+            raise OpoError(rc, "opo_create failed (no CUDA device, or unsupported grid)")
+
+    def _check(self, rc):
+        if rc:
+            raise OpoError(rc, lib().opo_last_error(self._h).decode())
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_field(self, which, arr):
+        a = np.ascontiguousarray(arr, dtype=np.complex128).reshape(-1)
+        self._check(lib().opo_set_field(self._h, which, a.ctypes.data_as(ctypes.c_void_p), MEM_HOST, FP64))
+
+    def set_field_device(self, which, ptr, precision):
+        self._check(lib().opo_set_field(self._h, which, ctypes.c_void_p(ptr), MEM_DEVICE, precision))
+
+    def get_field(self, which):
+        a = np.zeros(int(np.prod(self.shape)), dtype=np.complex128)
+        self._check(lib().opo_get_field(self._h, which, a.ctypes.data_as(ctypes.c_void_p), MEM_HOST, FP64))
+        return a.reshape(self.shape)
+
+    def get_field_device(self, which, ptr, precision):
+        self._check(lib().opo_get_field(self._h, which, ctypes.c_void_p(ptr), MEM_DEVICE, precision))
+
+    def run_single_pass(self):
+        self._check(lib().opo_run_single_pass(self._h))
+
+    def run_round_trips(self, n):
+        self._check(lib().opo_run_round_trips(self._h, n))
+
+    def field_sums(self):
+        s = np.zeros(3)
+        self._check(lib().opo_field_sums(self._h, _dptr(s)))
+        return s
+
+    def synchronize(self):
+        self._check(lib().opo_synchronize(self._h))
+
+    @property
+    def round_trip_index(self):
+        return lib().opo_round_trip_index(self._h)
+
+    @property
+    def kernel_launches(self):
+        return lib().opo_kernel_launches(self._h)
+
+    def close(self):
+        if self._h:
+            lib().opo_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+from .reference_api import Cavity, EFields, MgOsPPLT, PPLN, Solver  # noqa: E402,F401

@@ -1,0 +1,897 @@
+// Host side of the solver: FP64 physics of the reference classes (crystal, fields,
+// cavity), FFT stage plans, phase tables, the pass schedule of a single pass and of a
+// cavity round trip (captured as CUDA graphs), and the C-ABI of include/cuopo3d.h.
+
+#include "../../include/cuopo3d.h"
+#include "opo_internal.h"
+
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace {
+
+using cd = std::complex<double>;
+
+// Physical constants of the reference, DtypesConsts.cuh:55-57.
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kC = 299792458 * 1E6 / 1E12;           // um / ps
+constexpr double kEps0 = 8.8541878128E-12 * 1E12 / 1E6; // W ps / (V^2 um)
+
+// ---------------------------------------------------------------------------------
+// Sellmeier models.  Both reference crystals share one form
+//   n^2 = a0 + sum_r B_r / (L^2 - C_r^2) + d L^2,
+// (PPLN.cuh:97-117 with temperature-dependent B, C; MgOsPPLT.cuh:96-112), so that
+//   res_p(L) = sum_r B_r / (L^2 - C_r^2)^p,  R2 = res_2 - d,
+//   dn/dl = -L R2 / n, and the higher derivatives / GV / GVD / TOD follow the
+// reference expressions (PPLN.cuh:149-259, MgOsPPLT.cuh:138-226).
+struct Sellmeier {
+    double a0, d;
+    int nr;
+    double B[3], C2[3];  // C2 = C_r^2
+
+    double n(double L) const
+    {
+        double v = a0 + d * L * L;
+        for (int r = 0; r < nr; r++) v += B[r] / (L * L - C2[r]);
+        return std::sqrt(v);
+    }
+    double res(double L, int p) const
+    {
+        double v = 0;
+        for (int r = 0; r < nr; r++) v += B[r] / std::pow(L * L - C2[r], p);
+        return v;
+    }
+    double R2(double L) const { return res(L, 2) - d; }
+    double dn(double L) const { return -L * R2(L) / n(L); }
+    double d2n(double L) const
+    {
+        const double nn = n(L);
+        return (L * dn(L) / (nn * nn) - 1 / nn) * R2(L) + 4 * L * L / nn * res(L, 3);
+    }
+    double d3n(double L) const
+    {
+        const double nn = n(L), d1 = dn(L), d2 = d2n(L);
+        const double AA = ((2 * d1 + L * d2) / (nn * nn) - 2 * L * d1 * d1 / (nn * nn * nn)) * R2(L);
+        const double BB = (12 * L / nn - 4 * L * L / nn * d2 * (1 - 1 / nn)) * res(L, 3);
+        const double CC = -24 * L * L * L / nn * res(L, 4);
+        return AA + BB + CC;
+    }
+    double vg(double L) const { return kC / (n(L) - L * dn(L)); }
+    double gvd(double L) const { return std::pow(L, 3) * d2n(L) / (2 * kPi * kC * kC); }
+    double tod(double L) const
+    {
+        return -std::pow(L, 4) / (4 * kPi * kPi * kC * kC * kC) * (3 * d2n(L) + L * d3n(L));
+    }
+};
+
+struct CrystalModel {
+    Sellmeier s;
+    double d33;
+    double alpha[3];
+};
+
+bool crystal_model(int kind, double T, CrystalModel &m)
+{
+    if (kind == OPO_PPLN) {
+        // Jundt, congruent LiNbO3 (PPLN.cuh:100-115, 57-60): f = (T - 24.5)(T + 570.82)
+        const double f = (T - 24.5) * (T + 570.82);
+        const double G3 = 0.20692 + (-0.89e-8) * f;
+        m.s.a0 = 5.35583 + 4.629e-7 * f;
+        m.s.d = -1.5334e-2;
+        m.s.nr = 2;
+        m.s.B[0] = 0.100473 + 3.862e-8 * f; m.s.C2[0] = G3 * G3;
+        m.s.B[1] = 100.0 + 2.657e-5 * f;    m.s.C2[1] = 11.34927 * 11.34927;
+        m.d33 = 25.20e-6;
+        m.alpha[0] = 0.025e-4; m.alpha[1] = 0.002e-4; m.alpha[2] = 0.002e-4;
+        return true;
+    }
+    if (kind == OPO_MGOSPPLT) {
+        // Bruner, stoichiometric LiTaO3 (MgOsPPLT.cuh:99-110, 57-60)
+        const double TK2 = std::pow(T + 273.15, 2);
+        const double Cc = 0.185087 + 1.607839e-8 * TK2;
+        m.s.a0 = 4.502483;
+        m.s.d = -0.02357;
+        m.s.nr = 3;
+        m.s.B[0] = 0.007294 + 3.483933e-8 * TK2; m.s.C2[0] = Cc * Cc;
+        m.s.B[1] = 0.073423;                     m.s.C2[1] = 0.199595 * 0.199595;
+        m.s.B[2] = 0.001;                        m.s.C2[2] = 7.99724 * 7.99724;
+        m.d33 = 11.0e-6;
+        m.alpha[0] = 1.57e-4; m.alpha[1] = 0.17e-6; m.alpha[2] = 0.17e-6;
+        return true;
+    }
+    return false;
+}
+
+// Step count of the reference loop `for (real_t z = 0; z <= Lcr; z += dz)`
+// (Solver3D.cuh:949) in FP32 or FP64.
+int zloop_steps(double Lcr, double dz, bool f32)
+{
+    int n = 0;
+    if (f32) {
+        const float L = (float)Lcr, d = (float)dz;
+        for (float z = 0; z <= L; z += d) n++;
+    } else {
+        for (double z = 0; z <= Lcr; z += dz) n++;
+    }
+    return n;
+}
+
+// ---------------------------------------------------------------------------------
+// FFT stage plans and tables.
+
+bool split_pow2(int e, std::vector<int> &out)
+{
+    // radices for 2^e, largest first, balanced (16, 8, 4, 2)
+    static const int table[][3] = {{0, 0, 0}, {2, 0, 0}, {4, 0, 0}, {8, 0, 0}, {16, 0, 0}, {8, 4, 0},
+                                   {8, 8, 0}, {16, 8, 0}, {16, 16, 0}, {8, 8, 8}, {16, 8, 8}, {16, 16, 8},
+                                   {16, 16, 16}};
+    if (e < 0 || e > 12) return false;
+    for (int k = 0; k < 3; k++)
+        if (table[e][k]) out.push_back(table[e][k]);
+    return true;
+}
+
+// n = 2^a 3^b, first-stage radix r1 (a power of two dividing n).
+bool build_plan(int n, int r1_max, opo::AxisPlan &p, std::vector<cd> &tw)
+{
+    if (n < 4) return false;
+    int a = 0, b = 0, m = n;
+    while (m % 2 == 0) { m /= 2; a++; }
+    while (m % 3 == 0) { m /= 3; b++; }
+    if (m != 1) return false;
+    int r1 = 1, e1 = 0;
+    while (r1 * 2 <= r1_max && e1 < a) { r1 *= 2; e1++; }
+    // keep at least one more stage
+    while (e1 > 0 && n / r1 < 2) { r1 /= 2; e1--; }
+    if (r1 < 4 && a >= 2) { r1 = 4; e1 = 2; }
+    if (r1 < 4) return false;  // first stage needs a power-of-two radix >= 4
+    std::vector<int> rad;
+    rad.push_back(r1);
+    for (int k = 0; k < b; k++) rad.push_back(3);
+    if (!split_pow2(a - e1, rad)) return false;
+    if (rad.size() < 2 || (int)rad.size() > opo::kMaxStages) return false;
+    p.n = n;
+    p.ns = (int)rad.size();
+    tw.clear();
+    int L = n;
+    for (int s = 0; s < p.ns; s++) {
+        const int R = rad[s], q = L / R;
+        p.radix[s] = R;
+        p.len[s] = L;
+        p.twoff[s] = (int)tw.size();
+        for (int k = 1; k < R; k++)
+            for (int j = 0; j < q; j++) tw.push_back(std::polar(1.0, -2 * kPi * (double)j * k / L));
+        L = q;
+    }
+    return L == 1;
+}
+
+// Frequency bin held at position pos after the forward (decimation-in-frequency)
+// stages: pos = k1 (n/R1) + k2 (n/(R1 R2)) + ..., bin = k1 + R1 (k2 + R2 (k3 + ...)).
+int bin_of_position(const opo::AxisPlan &p, int pos)
+{
+    int w = p.n, bin = 0, mult = 1;
+    for (int s = 0; s < p.ns; s++) {
+        w /= p.radix[s];
+        const int k = pos / w;
+        pos -= k * w;
+        bin += k * mult;
+        mult *= p.radix[s];
+    }
+    return bin;
+}
+
+// Centred index of FFT bin i on an n-point grid after the reference's fftshift
+// (EFields3D.cuh:141-171): (i + n/2) mod n - n/2.
+double centred(int i, int n) { return (double)((i + n / 2) % n) - 0.5 * n; }
+
+// ---------------------------------------------------------------------------------
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+template <typename C> struct Tables {
+    C *tw_t = nullptr, *tw_x = nullptr, *tw_y = nullptr;
+    C *disp[3] = {};       // t: dispersion
+    C *gddm[3] = {};       // t: GDD compensation and mirror (signal, idler)
+    C *dx[3] = {}, *dy[3] = {};     // x, y: crystal diffraction
+    C *fx[3] = {}, *fy[3] = {};     // x, y: free-space return
+};
+
+}  // namespace
+
+struct OpoSolver {
+    OpoParams p{};
+    std::string err;
+    cudaStream_t stream = nullptr;
+    int dev = 0;
+    size_t V = 0;
+    size_t esz = 0;  // bytes per complex element
+    void *field[4] = {};  // Api, Ap, As, Ai
+    std::vector<void *> allocs;
+    opo::AxisPlan plan_t{}, plan_x{}, plan_y{};
+    int r1_t = 0, r1_x = 0, r1_y = 0;
+    opo::TileGeom geo_t{}, geo_x{}, geo_y{};
+    size_t smem_t = 0, smem_x = 0, smem_y = 0;
+    void *tables = nullptr;   // Tables<C>*
+    std::vector<double> w;
+    double *partials = nullptr, *sums_dev = nullptr;
+    int sum_blocks = 0;
+    void *staging = nullptr;  // conversion buffer (V complex of the other precision)
+    cudaGraphExec_t graph_rt[2] = {nullptr, nullptr};  // [last round trip?]
+    int rt_index = 0;
+    long long launches = 0;
+    int launches_rt[2] = {0, 0};
+    bool gdd_or_mirror = false;
+};
+
+namespace {
+
+const char *g_static_err = "";
+
+int fail(OpoSolver *s, int code, const std::string &msg)
+{
+    if (s) s->err = msg;
+    return code;
+}
+
+int cuda_fail(OpoSolver *s, cudaError_t e, const char *what)
+{
+    return fail(s, e == cudaErrorMemoryAllocation ? OPO_ERR_NOMEM : OPO_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define OPO_CU(s, call, what)                                   \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return cuda_fail((s), e_, what); \
+    } while (0)
+
+template <typename C> C to_c(const cd &v);
+template <> float2 to_c<float2>(const cd &v) { return make_float2((float)v.real(), (float)v.imag()); }
+template <> double2 to_c<double2>(const cd &v) { return make_double2(v.real(), v.imag()); }
+
+template <typename C> int upload(OpoSolver *s, const std::vector<cd> &h, C **out)
+{
+    std::vector<C> tmp(h.size());
+    for (size_t k = 0; k < h.size(); k++) tmp[k] = to_c<C>(h[k]);
+    void *d = nullptr;
+    OPO_CU(s, cudaMalloc(&d, sizeof(C) * tmp.size()), "cudaMalloc(table)");
+    s->allocs.push_back(d);
+    OPO_CU(s, cudaMemcpy(d, tmp.data(), sizeof(C) * tmp.size(), cudaMemcpyHostToDevice), "cudaMemcpy(table)");
+    *out = static_cast<C *>(d);
+    return OPO_OK;
+}
+
+int largest_divisor_leq(int n, int cap)
+{
+    if (cap < 1) return 0;
+    for (int d = cap < n ? cap : n; d >= 1; d--)
+        if (n % d == 0) return d;
+    return 1;
+}
+
+// Tile elements per field: 96 KB of shared memory for the three fields in either
+// precision, two CTAs per SM.
+size_t tile_elems(int precision) { return precision == OPO_FP64 ? 2048 : 4096; }
+
+template <typename C> int setup_tables(OpoSolver *s)
+{
+    const OpoParams &p = s->p;
+    auto *T = new (std::nothrow) Tables<C>();
+    if (!T) return fail(s, OPO_ERR_NOMEM, "host allocation");
+    s->tables = T;
+    std::vector<cd> twt, twx, twy;
+    const int r1max_t = sizeof(C) == 8 ? 16 : 8;
+    if (!build_plan(p.nt, r1max_t, s->plan_t, twt) || !build_plan(p.nx, 16, s->plan_x, twx) ||
+        !build_plan(p.ny, 16, s->plan_y, twy))
+        return fail(s, OPO_ERR_INVALID, "grid sizes must be 2^a 3^b and >= 4");
+    s->r1_t = s->plan_t.radix[0];
+    s->r1_x = s->plan_x.radix[0];
+    s->r1_y = s->plan_y.radix[0];
+    int rc;
+    if ((rc = upload<C>(s, twt, &T->tw_t)) || (rc = upload<C>(s, twx, &T->tw_x)) ||
+        (rc = upload<C>(s, twy, &T->tw_y)))
+        return rc;
+
+    const bool phys = (p.flags & OPO_PHYSICS) != 0;
+    const int nx = p.nx, ny = p.ny, nt = p.nt;
+    // t axis: dispersion exp(i dz w (vinv + w b2/2)) exp(-alpha dz/2) / nt
+    // (Solver3D.cuh:153-169; the 1/nt of the inverse transform folded in), placed at the
+    // digit-reversed positions of the t plan.
+    const double q2scale = (p.flags & OPO_ASIS_Q2) ? 1.0 / ((double)nx * ny) : 1.0;
+    for (int f = 0; f < 3; f++) {
+        std::vector<cd> tab(nt);
+        for (int pos = 0; pos < nt; pos++) {
+            const double wk = s->w[bin_of_position(s->plan_t, pos)];
+            cd v = std::polar(1.0, p.dz * wk * (p.vinv[f] + 0.5 * wk * p.beta2[f]));
+            if (!phys) v *= std::exp(-0.5 * p.alpha[f] * p.dz);
+            tab[pos] = v * (q2scale / nt);
+        }
+        if ((rc = upload<C>(s, tab, &T->disp[f]))) return rc;
+    }
+    // t axis at the end of a round trip, signal and idler: GDD compensation
+    // exp(i w^2 GDD / 2) (Solver3D.cuh:261-277, 676) times the mirror sqrt(R) e^{i phase}
+    // (Cavity3D.cuh:12-28) for resonant fields, / nt.
+    for (int f = 1; f < 3; f++) {
+        const bool res = (p.resonant >> f) & 1u;
+        const double R = f == 1 ? p.Rs : p.Ri;
+        const cd mirror = res ? std::sqrt(R) * std::polar(1.0, p.detuning) : cd(1, 0);
+        std::vector<cd> tab(nt);
+        for (int pos = 0; pos < nt; pos++) {
+            const double wk = s->w[bin_of_position(s->plan_t, pos)];
+            tab[pos] = std::polar(1.0, 0.5 * wk * wk * p.gdd) * mirror / (double)nt;
+        }
+        if ((rc = upload<C>(s, tab, &T->gddm[f]))) return rc;
+    }
+    // x, y: the diffraction propagator exp(sign L 2 pi^2 / k (fx^2 + fy^2)) of
+    // Solver3D.cuh:282-323 factorised as (x factor)(y factor); fx = centred(i) / (dx nx).
+    // The crystal y factor carries exp(-alpha dz / 2) and the 1/(nx ny) normalisation is
+    // split as 1/nx, 1/ny (shipped 1/(nx ny nt) with OPO_ASIS_Q1).
+    const double q1scale = (p.flags & OPO_ASIS_Q1) ? 1.0 / nt : 1.0;
+    for (int f = 0; f < 3; f++) {
+        const double cx = 2 * kPi * kPi / p.kdiff[f] / (p.dx * nx) / (p.dx * nx);
+        const double cy = 2 * kPi * kPi / p.kdiff[f] / (p.dy * ny) / (p.dy * ny);
+        std::vector<cd> tx(nx), ty(ny), ftx(nx), fty(ny);
+        for (int pos = 0; pos < nx; pos++) {
+            const double u = centred(bin_of_position(s->plan_x, pos), nx);
+            tx[pos] = std::polar(1.0, -p.dz * cx * u * u) / (double)nx;
+            ftx[pos] = std::polar(1.0, p.free_len * cx * u * u) / (double)nx;
+        }
+        for (int pos = 0; pos < ny; pos++) {
+            const double u = centred(bin_of_position(s->plan_y, pos), ny);
+            ty[pos] = std::polar(1.0, -p.dz * cy * u * u) * std::exp(-0.5 * p.alpha[f] * p.dz) *
+                      (q1scale / ny);
+            fty[pos] = std::polar(1.0, p.free_len * cy * u * u) / (double)ny;
+        }
+        if ((rc = upload<C>(s, tx, &T->dx[f])) || (rc = upload<C>(s, ty, &T->dy[f])) ||
+            (rc = upload<C>(s, ftx, &T->fx[f])) || (rc = upload<C>(s, fty, &T->fy[f])))
+            return rc;
+    }
+    s->gdd_or_mirror = p.gdd != 0 || (p.resonant & 6u);
+
+    // Tile geometry.
+    const size_t TE = tile_elems(p.precision);
+    const long long nxy = (long long)nx * ny;
+    {
+        const int P = largest_divisor_leq(nx, (int)(TE / nt));
+        if (P < 1 || (size_t)nt > TE) return fail(s, OPO_ERR_INVALID, "nt too large for one tile");
+        opo::TileGeom &g = s->geo_t;
+        g.nlines = P; g.LS = P; g.ntiles = (nx / P) * ny; g.tdiv = nx / P;
+        g.tmulA = P; g.tmulB = nx; g.gs_j = nxy; g.gs_l = 1;
+        s->smem_t = 3 * (size_t)nt * g.LS * sizeof(C);
+    }
+    {
+        const int Py = largest_divisor_leq(nx, (int)(TE / ny));
+        if (Py < 1 || (size_t)ny > TE) return fail(s, OPO_ERR_INVALID, "ny too large for one tile");
+        opo::TileGeom &g = s->geo_y;
+        g.nlines = Py; g.LS = Py; g.ntiles = (nx / Py) * nt; g.tdiv = nx / Py;
+        g.tmulA = Py; g.tmulB = nxy; g.gs_j = nx; g.gs_l = 1;
+        s->smem_y = 3 * (size_t)ny * g.LS * sizeof(C);
+    }
+    {
+        const int rows = largest_divisor_leq(ny * nt, (int)(TE / nx));
+        if (rows < 1 || (size_t)nx > TE) return fail(s, OPO_ERR_INVALID, "nx too large for one tile");
+        opo::TileGeom &g = s->geo_x;
+        g.nlines = rows;
+        // Pad the line stride so that the consecutive-butterfly mapping of the first
+        // and last stages is bank-conflict free: a conflict-free unit holds 128 B
+        // (16 complex64 or 8 complex128); with q' = min(nx/R1, unit) consecutive
+        // butterflies per line, LS = 0 mod (unit/q') makes b LS + l distinct.
+        const int unit = sizeof(C) == 8 ? 16 : 8;
+        int qq = nx / s->r1_x;
+        if (qq > unit) qq = unit;
+        const int step = unit / qq;
+        int LS = rows;
+        while ((LS % unit) != (step % unit)) LS++;
+        g.LS = LS;
+        g.ntiles = ny * nt / rows; g.tdiv = 1;
+        g.tmulA = 0; g.tmulB = (long long)rows * nx; g.gs_j = 1; g.gs_l = nx;
+        s->smem_x = 3 * (size_t)nx * g.LS * sizeof(C);
+    }
+    return OPO_OK;
+}
+
+template <typename C> C *fld(OpoSolver *s, int k) { return static_cast<C *>(s->field[k]); }
+
+// One t-pass.  n_rk4 half steps (z of each given), then, for the fields in tmask,
+// transform -> table -> inverse.
+template <typename C>
+int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, C *const *tab, unsigned tmask)
+{
+    const OpoParams &p = s->p;
+    opo::TPassArgs<C> a{};
+    using T = typename opo::TPassArgs<C>::T;
+    for (int f = 0; f < 3; f++) a.f[f] = fld<C>(s, f + 1);
+    a.psrc = reset_pump ? fld<C>(s, 0) : fld<C>(s, 1);
+    a.g = s->geo_t;
+    a.plan = s->plan_t;
+    auto *Tb = static_cast<Tables<C> *>(s->tables);
+    a.tw = Tb->tw_t;
+    for (int f = 0; f < 3; f++) a.tab[f] = tab ? tab[f] : nullptr;
+    a.tmask = tmask;
+    a.n_rk4 = n_rk4;
+    const bool phys = (p.flags & OPO_PHYSICS) != 0;
+    const double h = 0.5 * p.dz;
+    for (int f = 0; f < 3; f++) a.kappa[f] = (T)p.kappa[f];
+    a.c1 = (T)(phys ? 0.5 * h : 0.5);
+    a.c3 = (T)(phys ? h : 1.0);
+    a.h6 = (T)(h / 6.0);
+    a.use_phase = phys && p.dk != 0;
+    for (int k = 0; k < n_rk4 && k < 2; k++) {
+        // stage positions z, z + h/2, z + h (Solver3D.cuh:911-929 pass z, z+dz/4, z+dz/2)
+        const double zs[3] = {zh[k], zh[k] + 0.5 * h, zh[k] + h};
+        for (int j = 0; j < 3; j++) a.ph[k][j] = to_c<C>(std::polar(1.0, p.dk * zs[j]));
+    }
+    a.skip_rows = (p.flags & OPO_ASIS_Q2) ? 1 : 0;
+    a.nx = p.nx;
+    int grid = a.g.ntiles;
+    OPO_CU(s, opo::launch_tpass<C>(a, s->r1_t, grid, s->smem_t, s->stream), "t-pass launch");
+    s->launches++;
+    return OPO_OK;
+}
+
+template <typename C> int enqueue_axis(OpoSolver *s, bool xaxis, C *const *tab, unsigned mask)
+{
+    opo::AxisArgs<C> a{};
+    for (int f = 0; f < 3; f++) a.f[f] = fld<C>(s, f + 1);
+    auto *Tb = static_cast<Tables<C> *>(s->tables);
+    a.g = xaxis ? s->geo_x : s->geo_y;
+    a.plan = xaxis ? s->plan_x : s->plan_y;
+    a.tw = xaxis ? Tb->tw_x : Tb->tw_y;
+    for (int f = 0; f < 3; f++) a.tab[f] = tab[f];
+    a.tmask = mask;
+    const int r1 = xaxis ? s->r1_x : s->r1_y;
+    const size_t smem = xaxis ? s->smem_x : s->smem_y;
+    OPO_CU(s, opo::launch_axis<C>(a, r1, xaxis, a.g.ntiles, smem, s->stream), "axis-pass launch");
+    s->launches++;
+    return OPO_OK;
+}
+
+// z of the first half step of step k (ref: the loop variable; physics: k dz).
+double step_z(const OpoParams &p, int k) { return k * p.dz; }
+
+// The crystal: for k in [0, n): RK4(h) D F RK4(h) (Solver3D.cuh:946-960), with
+// D the t-axis operator and F the (x,y) one.  Passes: T(N D), X, Y, then for each
+// later step T(N N D), X, Y; the final N is left to the caller (end_pass).
+template <typename C> int enqueue_crystal(OpoSolver *s, bool reset_pump)
+{
+    const OpoParams &p = s->p;
+    auto *Tb = static_cast<Tables<C> *>(s->tables);
+    const bool disp = (p.flags & OPO_DISPERSION) != 0, diff = (p.flags & OPO_DIFFRACTION) != 0;
+    const bool phys = (p.flags & OPO_PHYSICS) != 0;
+    int rc;
+    for (int k = 0; k < p.n_steps; k++) {
+        double zh[2];
+        int nrk;
+        if (k == 0) {
+            zh[0] = step_z(p, 0);
+            nrk = 1;
+        } else {
+            zh[0] = phys ? step_z(p, k - 1) + 0.5 * p.dz : step_z(p, k - 1);
+            zh[1] = step_z(p, k);
+            nrk = 2;
+        }
+        if ((rc = enqueue_t<C>(s, reset_pump && k == 0, nrk, zh, Tb->disp, disp ? 7u : 0u))) return rc;
+        if (diff) {
+            if ((rc = enqueue_axis<C>(s, true, Tb->dx, 7u))) return rc;
+            if ((rc = enqueue_axis<C>(s, false, Tb->dy, 7u))) return rc;
+        }
+    }
+    return OPO_OK;
+}
+
+template <typename C> double last_half_z(const OpoParams &p)
+{
+    const int k = p.n_steps - 1;
+    return (p.flags & OPO_PHYSICS) ? step_z(p, k) + 0.5 * p.dz : step_z(p, k);
+}
+
+template <typename C> int enqueue_single_pass(OpoSolver *s)
+{
+    int rc;
+    if ((rc = enqueue_crystal<C>(s, false))) return rc;
+    const double z = last_half_z<C>(s->p);
+    return enqueue_t<C>(s, false, 1, &z, nullptr, 0u);
+}
+
+// One round trip (Solver3D.cuh:979-997): fresh pump, crystal, final half step fused
+// with GDD + mirrors on signal and idler (t-pass), then, unless this is the run's last
+// round trip, the free-space return of signal and idler (x and y passes).  The free
+// space and t-axis operators commute, so GDD + mirrors may precede the return.
+template <typename C> int enqueue_round_trip(OpoSolver *s, bool last)
+{
+    const OpoParams &p = s->p;
+    auto *Tb = static_cast<Tables<C> *>(s->tables);
+    int rc;
+    if ((rc = enqueue_crystal<C>(s, true))) return rc;
+    const double z = last_half_z<C>(p);
+    const bool disp = (p.flags & OPO_DISPERSION) != 0;
+    unsigned m = 0;
+    if (s->gdd_or_mirror) m = 6u;
+    if ((rc = enqueue_t<C>(s, false, 1, &z, Tb->gddm, m))) return rc;
+    (void)disp;
+    if (!last && (p.flags & OPO_DIFFRACTION)) {
+        if ((rc = enqueue_axis<C>(s, true, Tb->fx, 6u))) return rc;
+        if ((rc = enqueue_axis<C>(s, false, Tb->fy, 6u))) return rc;
+    }
+    return OPO_OK;
+}
+
+template <typename C> int build_graph(OpoSolver *s, bool last)
+{
+    cudaGraph_t g = nullptr;
+    OPO_CU(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    const long long before = s->launches;
+    int rc = enqueue_round_trip<C>(s, last);
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(s, e, "end capture");
+    s->launches_rt[last ? 1 : 0] = (int)(s->launches - before);
+    s->launches = before;
+    e = cudaGraphInstantiate(&s->graph_rt[last ? 1 : 0], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(s, e, "graph instantiate");
+    return OPO_OK;
+}
+
+template <typename C> int run_round_trips(OpoSolver *s, int n)
+{
+    for (int k = 0; k < n; k++) {
+        const bool last = s->rt_index == s->p.total_rt - 1;
+        const int gi = last ? 1 : 0;
+        if (!s->graph_rt[gi]) {
+            int rc = build_graph<C>(s, last);
+            if (rc) return rc;
+        }
+        OPO_CU(s, cudaGraphLaunch(s->graph_rt[gi], s->stream), "graph launch");
+        s->launches += s->launches_rt[gi];
+        s->rt_index++;
+    }
+    return OPO_OK;
+}
+
+template <typename C> int field_sums(OpoSolver *s, double out[3])
+{
+    OPO_CU(s, opo::launch_sums<C>(fld<C>(s, 1), fld<C>(s, 2), fld<C>(s, 3), s->V, s->partials, s->sum_blocks,
+                                  s->sums_dev, s->stream),
+           "sums launch");
+    s->launches += 2;
+    OPO_CU(s, cudaMemcpyAsync(out, s->sums_dev, 3 * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "sums copy");
+    OPO_CU(s, cudaStreamSynchronize(s->stream), "sums sync");
+    for (int k = 0; k < 3; k++)
+        if (!std::isfinite(out[k])) return fail(s, OPO_ERR_NONFINITE, "a field is not finite");
+    return OPO_OK;
+}
+
+bool valid_grid(int n) { return n >= 4; }
+
+}  // namespace
+
+// =================================================================================
+// C-ABI
+
+extern "C" {
+
+const char *opo_version(void) { return "cuopo3d-b200 0.1"; }
+
+int opo_crystal_dispersion(int crystal, double T, double L, double out[4])
+{
+    CrystalModel m;
+    if (!out || !crystal_model(crystal, T, m) || !(L > 0)) return OPO_ERR_INVALID;
+    out[0] = m.s.n(L);
+    out[1] = m.s.vg(L);
+    out[2] = m.s.gvd(L);
+    out[3] = m.s.tod(L);
+    return OPO_OK;
+}
+
+int opo_params_from_config(const OpoConfig *c, OpoParams *o, double *sc)
+{
+    if (!c || !o) return OPO_ERR_INVALID;
+    if (!valid_grid(c->nx) || !valid_grid(c->ny) || !valid_grid(c->nt) || c->nz < 2) return OPO_ERR_INVALID;
+    if (c->precision != OPO_FP32 && c->precision != OPO_FP64) return OPO_ERR_INVALID;
+    CrystalModel m;
+    if (!crystal_model(c->crystal, c->T, m)) return OPO_ERR_INVALID;
+    if (!(c->lp > 0) || !(c->ls > c->lp) || !(c->Lcr > 0) || !(c->LX > 0) || !(c->LY > 0)) return OPO_ERR_INVALID;
+    const double lp = c->lp, ls = c->ls, li = ls * lp / (ls - lp);  // cuOPO3D.cu:17
+    const double lam[3] = {lp, ls, li};
+    double n[3], v[3], b2[3], b3[3], alpha[3];
+    for (int f = 0; f < 3; f++) {
+        n[f] = m.s.n(lam[f]);
+        v[f] = m.s.vg(lam[f]);
+        b2[f] = m.s.gvd(lam[f]);
+        b3[f] = m.s.tod(lam[f]);
+        alpha[f] = c->alpha[f] >= 0 ? c->alpha[f] : m.alpha[f];
+    }
+    const double dQ = c->dQ > 0 ? c->dQ : 2.0 * m.d33 / kPi;
+    const double dx = c->LX / (c->nx - 1.0), dy = c->LY / (c->ny - 1.0), dz = c->Lcr / (c->nz - 1.0);
+    const bool phys = (c->flags & OPO_PHYSICS) != 0;
+    // EFields3D.cuh:222-224 (and the crystal constructors): kp = 2 pi ns / lp and
+    // ki = 2 pi ni / ls as shipped; corrected physics uses each wave's own n and lambda.
+    const double kp = phys ? 2.0 * kPi * n[0] / lp : 2.0 * kPi * n[1] / lp;
+    const double ks = 2.0 * kPi * n[1] / ls;
+    const double ki = phys ? 2.0 * kPi * n[2] / li : 2.0 * kPi * n[2] / ls;
+    const double dk = kp - ks - ki - 2.0 * kPi / c->Lambda;
+    const double Lcav = c->Lcav > 0 ? c->Lcav : 4 * c->Lcr;
+    const double trt = (Lcav + c->Lcr * (n[1] - 1)) / kC;  // Cavity3D.cuh:44
+    const double dt = trt / (c->nt - 1);
+    const int nsteps = c->n_steps > 0 ? c->n_steps : zloop_steps(c->Lcr, dz, c->zloop_f32 != 0);
+
+    std::memset(o, 0, sizeof(*o));
+    o->nx = c->nx; o->ny = c->ny; o->nt = c->nt; o->n_steps = nsteps;
+    o->flags = c->flags; o->precision = c->precision;
+    o->dz = (phys && c->n_steps > 0) ? c->Lcr / c->n_steps : dz;
+    o->Lcr = c->Lcr; o->dx = dx; o->dy = dy;
+    for (int f = 0; f < 3; f++) {
+        o->kappa[f] = 2 * kPi * dQ / (n[f] * lam[f]);  // EFields3D.cuh:219-221
+        o->beta2[f] = b2[f];
+        o->alpha[f] = alpha[f];
+    }
+    o->kdiff[0] = kp; o->kdiff[1] = ks; o->kdiff[2] = ki;
+    o->vinv[0] = 1 / v[0] - 1 / v[2];  // Solver3D.cuh:163-165
+    o->vinv[1] = 0.0;
+    o->vinv[2] = 1 / v[2] - 1 / v[1];
+    o->dk = dk;
+    o->Rs = c->Rs; o->Ri = c->Ri; o->detuning = c->detuning;
+    // Solver3D.cuh:676; GDD compensation exists only in the dispersion build (:476-480)
+    o->gdd = (c->gdd_gamma != 0 && (c->flags & OPO_DISPERSION)) ? -c->gdd_gamma * b2[1] * c->Lcr : 0.0;
+    o->free_len = c->Lcr;                                                // Solver3D.cuh:989
+    o->resonant = c->resonant;
+    o->total_rt = c->total_rt > 0 ? c->total_rt : 1;
+    o->t_window = c->t_window > 0 ? c->t_window : trt;
+    if (sc) {
+        const double vals[OPO_N_SCALARS] = {n[0], n[1], n[2], v[0], v[1], v[2], b2[0], b2[1], b2[2],
+                                            b3[0], b3[1], b3[2], dQ, dk, dx, dy, dz, kp, ks, ki,
+                                            o->kappa[0], o->kappa[1], o->kappa[2], trt, dt, (double)nsteps};
+        std::memcpy(sc, vals, sizeof(vals));
+    }
+    return OPO_OK;
+}
+
+int opo_time_freq(int nt, double T, double *t, double *w)
+{
+    if (nt < 2 || !(T > 0)) return OPO_ERR_INVALID;
+    // Common.cuh:120-128 linspace, EFields3D.cuh:58-68 fftshift, :322-325
+    for (int i = 0; t && i < nt; i++) t[i] = -T * 0.5 + i * (T * 0.5 - (-T * 0.5)) / (nt - 1);
+    if (w) {
+        const double fmin = -0.5 * nt / T, fmax = 0.5 * nt / T;
+        const int c = nt / 2;
+        for (int i = 0; i < nt; i++) {
+            const int src = i < c ? i + c : i - c;
+            w[i] = (fmin + src * (fmax - fmin) / (nt - 1)) * (2.0 * kPi);
+        }
+    }
+    return OPO_OK;
+}
+
+int opo_pump_field(const OpoConfig *c, double *Api)
+{
+    OpoParams p;
+    double sc[OPO_N_SCALARS];
+    int rc = opo_params_from_config(c, &p, sc);
+    if (rc) return rc;
+    if (!Api) return OPO_ERR_INVALID;
+    const int nx = c->nx, ny = c->ny, nt = c->nt;
+    std::vector<double> t(nt);
+    opo_time_freq(nt, p.t_window, t.data(), nullptr);
+    const double np_ = sc[0], dx = p.dx, dy = p.dy, P = c->P, w0 = c->w0, w02 = w0 * w0;
+    // EFields3D.cuh:247-253
+    const double tau = c->FWHM * std::sqrt(2.0) / (2 * std::sqrt(2 * std::log(2.0)));
+    const double zR = kPi * np_ * w02 / c->lp;
+    const double eta = c->focal / zR;
+    const double Ap0 = std::sqrt(4 * P / (kEps0 * kC * kPi * np_ * w02));
+    const cd MX(1, -eta);
+    // sech^2 intensity envelope (new): FWHM = 2 acosh(sqrt 2) ts; P is the window-average
+    // power, so the peak power is P T / (2 ts).
+    const double ts = c->FWHM / (2 * std::acosh(std::sqrt(2.0)));
+    const double Ap0s = std::sqrt(4 * (P * p.t_window / (2 * ts)) / (kEps0 * kC * kPi * np_ * w02));
+    const double uX = 0.5 * nx, uY = 0.5 * ny;
+    for (int it = 0; it < nt; it++) {
+        const double tn = t[it] / tau;
+        for (int y = 0; y < ny; y++)
+            for (int x = 0; x < nx; x++) {
+                const double rx = (x - uX) * dx, ry = (y - uY) * dy, r2 = rx * rx + ry * ry;
+                const cd foc = (Ap0 / MX) * std::exp(cd(-r2, 0) / (w02 * MX));  // EFields3D.cuh:115
+                cd v;
+                switch (c->pump_mode) {
+                case OPO_PUMP_WAVEPLANE_CW: v = Ap0 * std::exp(-r2 / w02); break;            // :79
+                case OPO_PUMP_WAVEPLANE_PULSED: v = Ap0 * std::exp(-tn * tn - r2 / w02); break; // :96
+                case OPO_PUMP_FOCUSED_CW: v = foc; break;
+                case OPO_PUMP_FOCUSED_PULSED: v = foc * std::exp(-tn * tn); break;          // :132
+                case OPO_PUMP_FOCUSED_SECH2: v = foc * (Ap0s / Ap0) / std::cosh(t[it] / ts); break;
+                case OPO_PUMP_WAVEPLANE_SECH2: v = Ap0s * std::exp(-r2 / w02) / std::cosh(t[it] / ts); break;
+                default: return OPO_ERR_INVALID;
+                }
+                const size_t id = (size_t)it * nx * ny + (size_t)y * nx + x;
+                Api[2 * id] = v.real();
+                Api[2 * id + 1] = v.imag();
+            }
+    }
+    return OPO_OK;
+}
+
+int opo_noise(uint64_t seed, double sigma, size_t n, double *out)
+{
+    if (!out) return OPO_ERR_INVALID;
+    for (size_t v = 0; v < 2 * n; v++) {
+        double acc = 0;
+        for (int j = 0; j < 12; j++) {
+            uint64_t z = seed + 0x9E3779B97F4A7C15ull * (uint64_t)(12 * v + j + 1);
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+            z ^= z >> 31;
+            acc += (double)(z >> 11) * 0x1.0p-53;
+        }
+        out[v] = sigma * (acc - 6.0);
+    }
+    return OPO_OK;
+}
+
+int opo_create(const OpoParams *p, const double *w, OpoSolver **out)
+{
+    if (!out) return OPO_ERR_INVALID;
+    *out = nullptr;
+    if (!p || !w) return OPO_ERR_INVALID;
+    if (p->precision != OPO_FP32 && p->precision != OPO_FP64) return OPO_ERR_INVALID;
+    if (!valid_grid(p->nx) || !valid_grid(p->ny) || !valid_grid(p->nt) || p->n_steps < 1) return OPO_ERR_INVALID;
+    OpoSolver *s = new (std::nothrow) OpoSolver();
+    if (!s) return OPO_ERR_NOMEM;
+    s->p = *p;
+    if (s->p.total_rt < 1) s->p.total_rt = 1;
+    s->w.assign(w, w + p->nt);
+    s->V = (size_t)p->nx * p->ny * p->nt;
+    s->esz = p->precision == OPO_FP64 ? sizeof(double2) : sizeof(float2);
+    int rc = OPO_OK;
+    cudaError_t e;
+    do {
+        if ((e = cudaGetDevice(&s->dev)) != cudaSuccess) { rc = cuda_fail(s, e, "cudaGetDevice"); break; }
+        if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+            rc = cuda_fail(s, e, "stream");
+            break;
+        }
+        for (int k = 0; k < 4 && !rc; k++) {
+            if ((e = cudaMalloc(&s->field[k], s->esz * s->V)) != cudaSuccess) rc = cuda_fail(s, e, "cudaMalloc(field)");
+            else if ((e = cudaMemset(s->field[k], 0, s->esz * s->V)) != cudaSuccess) rc = cuda_fail(s, e, "memset");
+        }
+        if (rc) break;
+        rc = p->precision == OPO_FP64 ? setup_tables<double2>(s) : setup_tables<float2>(s);
+        if (rc) break;
+        size_t mx = s->smem_t;
+        if (s->smem_x > mx) mx = s->smem_x;
+        if (s->smem_y > mx) mx = s->smem_y;
+        if (mx > 227 * 1024) { rc = fail(s, OPO_ERR_INVALID, "tile does not fit in shared memory"); break; }
+        if ((e = opo::configure_kernels(96 * 1024 > mx ? 96 * 1024 : mx)) != cudaSuccess) {
+            rc = cuda_fail(s, e, "configure kernels");
+            break;
+        }
+        s->sum_blocks = 148 * 4;
+        if ((e = cudaMalloc((void **)&s->partials, sizeof(double) * 3 * (s->sum_blocks + 1))) != cudaSuccess) {
+            rc = cuda_fail(s, e, "cudaMalloc(partials)");
+            break;
+        }
+        s->sums_dev = s->partials + 3 * s->sum_blocks;
+    } while (0);
+    if (rc) {
+        g_static_err = "opo_create failed";
+        std::fprintf(stderr, "opo_create: %s\n", s->err.c_str());
+        opo_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return OPO_OK;
+}
+
+void opo_destroy(OpoSolver *s)
+{
+    if (!s) return;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (auto &g : s->graph_rt)
+        if (g) cudaGraphExecDestroy(g);
+    for (auto *pp : s->allocs) cudaFree(pp);
+    for (auto *f : s->field)
+        if (f) cudaFree(f);
+    if (s->partials) cudaFree(s->partials);
+    if (s->staging) cudaFree(s->staging);
+    if (s->tables) {
+        if (s->p.precision == OPO_FP64) delete static_cast<Tables<double2> *>(s->tables);
+        else delete static_cast<Tables<float2> *>(s->tables);
+    }
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+static int ensure_staging(OpoSolver *s)
+{
+    if (s->staging) return OPO_OK;
+    OPO_CU(s, cudaMalloc(&s->staging, sizeof(double2) * s->V), "cudaMalloc(staging)");
+    return OPO_OK;
+}
+
+int opo_set_field(OpoSolver *s, int which, const void *src, int where, int prec)
+{
+    if (!s) return OPO_ERR_INVALID;
+    if (which < 0 || which > 3 || !src || (where != OPO_MEM_HOST && where != OPO_MEM_DEVICE) ||
+        (prec != OPO_FP32 && prec != OPO_FP64))
+        return fail(s, OPO_ERR_INVALID, "opo_set_field: bad argument");
+    const cudaMemcpyKind kind = where == OPO_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    if (prec == s->p.precision) {
+        OPO_CU(s, cudaMemcpyAsync(s->field[which], src, s->esz * s->V, kind, s->stream), "set_field copy");
+        return OPO_OK;
+    }
+    int rc = ensure_staging(s);
+    if (rc) return rc;
+    const size_t sbytes = (prec == OPO_FP64 ? sizeof(double2) : sizeof(float2)) * s->V;
+    OPO_CU(s, cudaMemcpyAsync(s->staging, src, sbytes, kind, s->stream), "set_field staging copy");
+    if (prec == OPO_FP64)
+        OPO_CU(s, opo::launch_convert_d2f((const double2 *)s->staging, (float2 *)s->field[which], s->V, s->stream), "convert");
+    else
+        OPO_CU(s, opo::launch_convert_f2d((const float2 *)s->staging, (double2 *)s->field[which], s->V, s->stream), "convert");
+    s->launches++;
+    return OPO_OK;
+}
+
+int opo_get_field(OpoSolver *s, int which, void *dst, int where, int prec)
+{
+    if (!s) return OPO_ERR_INVALID;
+    if (which < 0 || which > 3 || !dst || (where != OPO_MEM_HOST && where != OPO_MEM_DEVICE) ||
+        (prec != OPO_FP32 && prec != OPO_FP64))
+        return fail(s, OPO_ERR_INVALID, "opo_get_field: bad argument");
+    const cudaMemcpyKind kind = where == OPO_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (prec == s->p.precision) {
+        OPO_CU(s, cudaMemcpyAsync(dst, s->field[which], s->esz * s->V, kind, s->stream), "get_field copy");
+    } else {
+        int rc = ensure_staging(s);
+        if (rc) return rc;
+        const size_t dbytes = (prec == OPO_FP64 ? sizeof(double2) : sizeof(float2)) * s->V;
+        if (prec == OPO_FP64)
+            OPO_CU(s, opo::launch_convert_f2d((const float2 *)s->field[which], (double2 *)s->staging, s->V, s->stream), "convert");
+        else
+            OPO_CU(s, opo::launch_convert_d2f((const double2 *)s->field[which], (float2 *)s->staging, s->V, s->stream), "convert");
+        s->launches++;
+        OPO_CU(s, cudaMemcpyAsync(dst, s->staging, dbytes, kind, s->stream), "get_field staging copy");
+    }
+    if (where == OPO_MEM_HOST) OPO_CU(s, cudaStreamSynchronize(s->stream), "get_field sync");
+    return OPO_OK;
+}
+
+int opo_run_single_pass(OpoSolver *s)
+{
+    if (!s) return OPO_ERR_INVALID;
+    return s->p.precision == OPO_FP64 ? enqueue_single_pass<double2>(s) : enqueue_single_pass<float2>(s);
+}
+
+int opo_run_round_trips(OpoSolver *s, int n)
+{
+    if (!s || n < 0) return s ? fail(s, OPO_ERR_INVALID, "negative round-trip count") : OPO_ERR_INVALID;
+    return s->p.precision == OPO_FP64 ? run_round_trips<double2>(s, n) : run_round_trips<float2>(s, n);
+}
+
+int opo_field_sums(OpoSolver *s, double sums[3])
+{
+    if (!s || !sums) return s ? fail(s, OPO_ERR_INVALID, "null output") : OPO_ERR_INVALID;
+    return s->p.precision == OPO_FP64 ? field_sums<double2>(s, sums) : field_sums<float2>(s, sums);
+}
+
+int opo_synchronize(OpoSolver *s)
+{
+    if (!s) return OPO_ERR_INVALID;
+    OPO_CU(s, cudaStreamSynchronize(s->stream), "synchronize");
+    return OPO_OK;
+}
+
+int opo_round_trip_index(const OpoSolver *s) { return s ? s->rt_index : -1; }
+long long opo_kernel_launches(const OpoSolver *s) { return s ? s->launches : -1; }
+const char *opo_last_error(const OpoSolver *s) { return s ? s->err.c_str() : g_static_err; }
+
+}  // extern "C"

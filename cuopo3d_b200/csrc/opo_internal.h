@@ -1,0 +1,84 @@
+// Internal types shared by the host schedule (opo_host.cu) and the pass kernels
+// (ssfm_kernels.cu).  Not part of the C-ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+namespace opo {
+
+constexpr int kMaxStages = 8;
+constexpr int kThreads = 256;        // threads per CTA of every pass kernel
+
+// In-place line FFT of length n done in `ns` stages.  Forward stages are decimation in
+// frequency: stage s splits sub-sequences of length len[s] with radix radix[s]
+// (len[0] = n, len[s+1] = len[s] / radix[s], len[ns-1] = radix[ns-1]); the output is
+// in mixed-radix digit-reversed order, which the phase tables are permuted to match,
+// and the inverse stages (decimation in time, reverse order) restore natural order.
+// Stage s twiddles W_len^{j k} = exp(-2 pi i j k / len) sit at tw[twoff[s] + (k-1) q + j],
+// q = len / radix, k in [1, radix), j in [0, q).
+struct AxisPlan {
+    int n;
+    int ns;
+    int radix[kMaxStages];
+    int len[kMaxStages];
+    int twoff[kMaxStages];
+};
+
+// Placement of one tile of lines.  Line l, element j of tile `tile` is the global
+// element  base(tile) + j * gs_j + l * gs_l  with
+//   base(tile) = (tile % tdiv) * tmulA + (tile / tdiv) * tmulB,
+// and lives in shared memory at  j * LS + l  (one such block per field).
+struct TileGeom {
+    int nlines;
+    int LS;
+    int ntiles;
+    int tdiv;
+    long long tmulA, tmulB;
+    long long gs_j, gs_l;
+};
+
+template <typename C> struct RealOf;
+template <> struct RealOf<float2> { using type = float; };
+template <> struct RealOf<double2> { using type = double; };
+
+template <typename C> struct TPassArgs {
+    using T = typename RealOf<C>::type;
+    C *f[3];            // pump, signal, idler (updated in place)
+    const C *psrc;      // pump source: Api when the pass starts a round trip, else f[0]
+    TileGeom g;
+    AxisPlan plan;
+    const C *tw;        // stage twiddles of the t axis
+    const C *tab[3];    // phase table per field (digit-reversed order), used when in tmask
+    unsigned tmask;     // fields that get the t-axis transform
+    int n_rk4;          // coupled-wave half steps before the transform (0, 1, 2)
+    int use_phase;      // apply exp(-/+ i dk z) (corrected physics)
+    T kappa[3];
+    T c1, c3, h6;       // RK4 stage offsets (k1, k2 -> c1; k3 -> c3) and final weight h/6
+    C ph[2][3];         // exp(i dk z) at the stage positions z, z+h/2, z+h of each half step
+    int skip_rows;      // shipped quirk: transform only row y = 0 (tiles with y != 0 skip)
+    int nx;             // grid width (for the row test above)
+};
+
+template <typename C> struct AxisArgs {
+    C *f[3];
+    TileGeom g;
+    AxisPlan plan;
+    const C *tw;
+    const C *tab[3];
+    unsigned tmask;
+};
+
+// Launchers (ssfm_kernels.cu).  smem in bytes; grid = number of CTAs.
+template <typename C> cudaError_t launch_tpass(const TPassArgs<C> &a, int r1, int grid, size_t smem,
+                                               cudaStream_t st);
+template <typename C> cudaError_t launch_axis(const AxisArgs<C> &a, int r1, bool bfast, int grid,
+                                              size_t smem, cudaStream_t st);
+template <typename C> cudaError_t launch_sums(const C *f0, const C *f1, const C *f2, size_t n,
+                                              double *partials, int nblocks, double *out,
+                                              cudaStream_t st);
+cudaError_t launch_convert_d2f(const double2 *src, float2 *dst, size_t n, cudaStream_t st);
+cudaError_t launch_convert_f2d(const float2 *src, double2 *dst, size_t n, cudaStream_t st);
+cudaError_t configure_kernels(size_t max_smem);
+
+}  // namespace opo

@@ -1,0 +1,509 @@
+// Pass kernels of the split-step solver for sm_100a.
+//
+// Every z-step of the reference (Solver3D.cuh:946-960: RK4(dz/2), dispersion,
+// diffraction, RK4(dz/2)) is executed as three passes over the resident fields, each
+// reading and writing the three complex fields once:
+//   t-pass    coupled-wave RK4 half steps (all stages in registers) fused with the
+//             t-axis operator: transform, times the dispersion phase, inverse transform
+//   x-pass,   the separable diffraction operator exp(-i dz 2 pi^2 (fx^2 + fy^2) / k)
+//   y-pass    = (x factor) (y factor), one axis per pass.
+// A CTA owns a tile of whole lines of one axis for all three fields: lines are staged
+// in shared memory with the line index fastest (so every stage is bank-conflict free),
+// the first transform stage is fused with the coalesced global load (and, in the
+// t-pass, with the RK4 update) and the last inverse stage with the global store.  The
+// middle stages exchange through shared memory; the last forward stage, the phase
+// multiply and the first inverse stage are one register-resident step.
+
+#include "fft_radix.cuh"
+#include "opo_internal.h"
+
+namespace opo {
+
+template <int S, typename C> __device__ __forceinline__ C twmul(C x, C w)
+{
+    // w holds exp(-2 pi i e / L); a stage of sign S multiplies by exp(S 2 pi i e / L)
+    return S < 0 ? cmul(x, w) : cmulc(x, w);
+}
+
+__device__ __forceinline__ long long tile_base(const TileGeom &g, int tile)
+{
+    return (long long)(tile % g.tdiv) * g.tmulA + (long long)(tile / g.tdiv) * g.tmulB;
+}
+
+// ---------------------------------------------------------------------------------
+// Shared-memory stages.  Work item w -> (line l fastest, butterfly b, field slot f).
+
+template <typename C, int R, int S, bool DIT>
+__device__ void smem_stage(C *sm, int LS, int nlines, int n, int L, const C *tw, int nf,
+                           const int *fslot)
+{
+    const int q = L / R, nb = n / R;
+    const int per_field = nb * nlines;
+    for (int w = threadIdx.x; w < per_field * nf; w += blockDim.x) {
+        const int f = w / per_field, r = w - f * per_field;
+        const int b = r / nlines, l = r - b * nlines;
+        const int g = b / q, j = b - g * q, base = g * L + j;
+        C *s = sm + (size_t)fslot[f] * n * LS + l;
+        C x[R];
+#pragma unroll
+        for (int m = 0; m < R; m++) x[m] = s[(base + m * q) * LS];
+        if (DIT && q > 1) {
+#pragma unroll
+            for (int m = 1; m < R; m++) x[m] = twmul<S>(x[m], __ldg(tw + (m - 1) * q + j));
+        }
+        dft<R, S>(x);
+        if (!DIT && q > 1) {
+#pragma unroll
+            for (int k = 1; k < R; k++) x[k] = twmul<S>(x[k], __ldg(tw + (k - 1) * q + j));
+        }
+#pragma unroll
+        for (int k = 0; k < R; k++) s[(base + k * q) * LS] = x[k];
+    }
+}
+
+// Last forward stage (q = 1), phase multiply, first inverse stage, in registers.
+template <typename C, int R, int SF>
+__device__ void fused_middle(C *sm, int LS, int nlines, int n, const C *const *tab, int nf,
+                             const int *fslot, const int *fid)
+{
+    const int nb = n / R;
+    const int per_field = nb * nlines;
+    for (int w = threadIdx.x; w < per_field * nf; w += blockDim.x) {
+        const int f = w / per_field, r = w - f * per_field;
+        const int g = r / nlines, l = r - g * nlines;
+        C *s = sm + (size_t)fslot[f] * n * LS + l;
+        const C *tb = tab[fid[f]] + g * R;
+        C x[R];
+#pragma unroll
+        for (int m = 0; m < R; m++) x[m] = s[(g * R + m) * LS];
+        dft<R, SF>(x);
+#pragma unroll
+        for (int k = 0; k < R; k++) x[k] = cmul(x[k], __ldg(tb + k));
+        dft<R, -SF>(x);
+#pragma unroll
+        for (int k = 0; k < R; k++) s[(g * R + k) * LS] = x[k];
+    }
+}
+
+template <typename C, int S, bool DIT>
+__device__ void smem_stage_dispatch(int R, C *sm, int LS, int nlines, int n, int L, const C *tw,
+                                    int nf, const int *fslot)
+{
+    switch (R) {
+    case 2: smem_stage<C, 2, S, DIT>(sm, LS, nlines, n, L, tw, nf, fslot); break;
+    case 3: smem_stage<C, 3, S, DIT>(sm, LS, nlines, n, L, tw, nf, fslot); break;
+    case 4: smem_stage<C, 4, S, DIT>(sm, LS, nlines, n, L, tw, nf, fslot); break;
+    case 8: smem_stage<C, 8, S, DIT>(sm, LS, nlines, n, L, tw, nf, fslot); break;
+    case 16: smem_stage<C, 16, S, DIT>(sm, LS, nlines, n, L, tw, nf, fslot); break;
+    default: break;
+    }
+}
+
+template <typename C, int SF>
+__device__ void fused_dispatch(int R, C *sm, int LS, int nlines, int n, const C *const *tab,
+                               int nf, const int *fslot, const int *fid)
+{
+    switch (R) {
+    case 2: fused_middle<C, 2, SF>(sm, LS, nlines, n, tab, nf, fslot, fid); break;
+    case 3: fused_middle<C, 3, SF>(sm, LS, nlines, n, tab, nf, fslot, fid); break;
+    case 4: fused_middle<C, 4, SF>(sm, LS, nlines, n, tab, nf, fslot, fid); break;
+    case 8: fused_middle<C, 8, SF>(sm, LS, nlines, n, tab, nf, fslot, fid); break;
+    case 16: fused_middle<C, 16, SF>(sm, LS, nlines, n, tab, nf, fslot, fid); break;
+    default: break;
+    }
+}
+
+// Stages 1 .. ns-1 forward, fused middle, inverse back to stage 1 (stage 0 is fused
+// with the global load / store by the caller).
+template <typename C, int SF>
+__device__ void middle_stages(C *sm, const TileGeom &g, const AxisPlan &p, const C *tw,
+                              const C *const *tab, int nf, const int *fslot, const int *fid)
+{
+    for (int s = 1; s < p.ns - 1; s++) {
+        smem_stage_dispatch<C, SF, false>(p.radix[s], sm, g.LS, g.nlines, p.n, p.len[s],
+                                          tw + p.twoff[s], nf, fslot);
+        __syncthreads();
+    }
+    fused_dispatch<C, SF>(p.radix[p.ns - 1], sm, g.LS, g.nlines, p.n, tab, nf, fslot, fid);
+    __syncthreads();
+    for (int s = p.ns - 2; s >= 1; s--) {
+        smem_stage_dispatch<C, -SF, true>(p.radix[s], sm, g.LS, g.nlines, p.n, p.len[s],
+                                          tw + p.twoff[s], nf, fslot);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Coupled-wave equations, reference Solver3D.cuh:365-425 and :872-943.
+//   dAp = i kp As Ai e^{-i dk z}, dAs = i ks Ap Ai* e^{i dk z}, dAi = i ki Ap As* e^{i dk z}
+// One half step of size h = dz/2: k1 = f(A), k2 = f(A + c1 k1), k3 = f(A + c1 k2),
+// k4 = f(A + c3 k3), A += (k1 + 2 k2 + 2 k3 + k4) h / 6.  The shipped stage offsets are
+// c1 = 0.5, c3 = 1 (no step size); corrected physics uses c1 = h/2, c3 = h.
+
+template <typename C, typename T>
+__device__ __forceinline__ void cwe_rhs(const T *kap, C p, C s, C i, C &dp, C &ds, C &di)
+{
+    C si = cmul(s, i), pic = cmulc(p, i), psc = cmulc(p, s);
+    dp = C{-kap[0] * si.y, kap[0] * si.x};
+    ds = C{-kap[1] * pic.y, kap[1] * pic.x};
+    di = C{-kap[2] * psc.y, kap[2] * psc.x};
+}
+
+template <typename C, typename T>
+__device__ __forceinline__ void cwe_rhs_phase(const T *kap, const C &ph, C p, C s, C i, C &dp, C &ds,
+                                              C &di)
+{
+    cwe_rhs(kap, p, s, i, dp, ds, di);
+    dp = cmulc(dp, ph);
+    ds = cmul(ds, ph);
+    di = cmul(di, ph);
+}
+
+template <typename C>
+__device__ __forceinline__ void rk4_half(const TPassArgs<C> &a, int h, C &p, C &s, C &i)
+{
+    using T = typename TPassArgs<C>::T;
+    C k1p, k1s, k1i, k2p, k2s, k2i, k3p, k3s, k3i, k4p, k4s, k4i;
+    const T c1 = a.c1, c3 = a.c3;
+    if (!a.use_phase) {
+        cwe_rhs(a.kappa, p, s, i, k1p, k1s, k1i);
+        cwe_rhs(a.kappa, C{p.x + c1 * k1p.x, p.y + c1 * k1p.y}, C{s.x + c1 * k1s.x, s.y + c1 * k1s.y},
+                C{i.x + c1 * k1i.x, i.y + c1 * k1i.y}, k2p, k2s, k2i);
+        cwe_rhs(a.kappa, C{p.x + c1 * k2p.x, p.y + c1 * k2p.y}, C{s.x + c1 * k2s.x, s.y + c1 * k2s.y},
+                C{i.x + c1 * k2i.x, i.y + c1 * k2i.y}, k3p, k3s, k3i);
+        cwe_rhs(a.kappa, C{p.x + c3 * k3p.x, p.y + c3 * k3p.y}, C{s.x + c3 * k3s.x, s.y + c3 * k3s.y},
+                C{i.x + c3 * k3i.x, i.y + c3 * k3i.y}, k4p, k4s, k4i);
+    } else {
+        const C *ph = a.ph[h];
+        cwe_rhs_phase(a.kappa, ph[0], p, s, i, k1p, k1s, k1i);
+        cwe_rhs_phase(a.kappa, ph[1], C{p.x + c1 * k1p.x, p.y + c1 * k1p.y},
+                      C{s.x + c1 * k1s.x, s.y + c1 * k1s.y}, C{i.x + c1 * k1i.x, i.y + c1 * k1i.y},
+                      k2p, k2s, k2i);
+        cwe_rhs_phase(a.kappa, ph[1], C{p.x + c1 * k2p.x, p.y + c1 * k2p.y},
+                      C{s.x + c1 * k2s.x, s.y + c1 * k2s.y}, C{i.x + c1 * k2i.x, i.y + c1 * k2i.y},
+                      k3p, k3s, k3i);
+        cwe_rhs_phase(a.kappa, ph[2], C{p.x + c3 * k3p.x, p.y + c3 * k3p.y},
+                      C{s.x + c3 * k3s.x, s.y + c3 * k3s.y}, C{i.x + c3 * k3i.x, i.y + c3 * k3i.y},
+                      k4p, k4s, k4i);
+    }
+    const T w = a.h6;
+    p.x += (k1p.x + T(2) * k2p.x + T(2) * k3p.x + k4p.x) * w;
+    p.y += (k1p.y + T(2) * k2p.y + T(2) * k3p.y + k4p.y) * w;
+    s.x += (k1s.x + T(2) * k2s.x + T(2) * k3s.x + k4s.x) * w;
+    s.y += (k1s.y + T(2) * k2s.y + T(2) * k3s.y + k4s.y) * w;
+    i.x += (k1i.x + T(2) * k2i.x + T(2) * k3i.x + k4i.x) * w;
+    i.y += (k1i.y + T(2) * k2i.y + T(2) * k3i.y + k4i.y) * w;
+}
+
+// ---------------------------------------------------------------------------------
+// t-pass: tile = P consecutive pixels (x) of one row y, all t, all three fields.
+// Stage 0 (radix R1, stride q = nt/R1): each thread loads R1 time samples of one pixel
+// for p, s, i, applies n_rk4 half steps to each voxel, then the first forward stage of
+// every transformed field into shared memory (untransformed fields go straight back).
+
+template <typename C, int R1>
+__global__ void __launch_bounds__(kThreads) tpass_kernel(TPassArgs<C> a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *sm = reinterpret_cast<C *>(smem_raw);
+    const AxisPlan &p = a.plan;
+    const TileGeom &g = a.g;
+    const int n = p.n, q = n / R1, P = g.nlines, LS = g.LS;
+    int fslot[3], fid[3], nf = 0;
+    for (int f = 0; f < 3; f++)
+        if (a.tmask & (1u << f)) { fslot[nf] = nf; fid[nf] = f; nf++; }
+
+    for (int tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
+        const long long base = tile_base(g, tile);
+        bool xform = nf > 0;
+        if (a.skip_rows && (base / a.nx) % (g.gs_j / a.nx) != 0) xform = false;
+        for (int w = threadIdx.x; w < q * P; w += blockDim.x) {
+            const int b = w / P, l = w - b * P;
+            const long long gb = base + (long long)l * g.gs_l + (long long)b * g.gs_j;
+            C x[3][R1];
+#pragma unroll
+            for (int m = 0; m < R1; m++) {
+                const long long gi = gb + (long long)m * q * g.gs_j;
+                x[0][m] = a.psrc[gi];
+                x[1][m] = a.f[1][gi];
+                x[2][m] = a.f[2][gi];
+            }
+            for (int h = 0; h < a.n_rk4; h++) {
+#pragma unroll
+                for (int m = 0; m < R1; m++) rk4_half(a, h, x[0][m], x[1][m], x[2][m]);
+            }
+            int slot = 0;
+#pragma unroll
+            for (int f = 0; f < 3; f++) {
+                if (xform && (a.tmask & (1u << f))) {
+                    dft<R1, +1>(x[f]);
+#pragma unroll
+                    for (int k = 1; k < R1; k++) x[f][k] = twmul<+1>(x[f][k], __ldg(a.tw + (k - 1) * q + b));
+                    C *s = sm + (size_t)slot * n * LS + l;
+#pragma unroll
+                    for (int k = 0; k < R1; k++) s[(b + k * q) * LS] = x[f][k];
+                    slot++;
+                } else {
+#pragma unroll
+                    for (int m = 0; m < R1; m++) a.f[f][gb + (long long)m * q * g.gs_j] = x[f][m];
+                }
+            }
+        }
+        if (!xform) continue;
+        __syncthreads();
+        middle_stages<C, +1>(sm, g, p, a.tw, a.tab, nf, fslot, fid);
+        // Stage 0 inverse (sign -1) and store.
+        for (int w = threadIdx.x; w < q * P * nf; w += blockDim.x) {
+            const int f = w / (q * P), r = w - f * (q * P);
+            const int b = r / P, l = r - b * P;
+            C *s = sm + (size_t)fslot[f] * n * LS + l;
+            C x[R1];
+#pragma unroll
+            for (int m = 0; m < R1; m++) x[m] = s[(b + m * q) * LS];
+#pragma unroll
+            for (int m = 1; m < R1; m++) x[m] = twmul<-1>(x[m], __ldg(a.tw + (m - 1) * q + b));
+            dft<R1, -1>(x);
+            C *dst = a.f[fid[f]] + base + (long long)l * g.gs_l + (long long)b * g.gs_j;
+#pragma unroll
+            for (int k = 0; k < R1; k++) dst[(long long)k * q * g.gs_j] = x[k];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Axis pass (x or y diffraction factor): forward transform sign -1 (the reference's
+// CUFFT_FORWARD), phase, inverse sign +1.  BFAST maps consecutive threads to
+// consecutive butterflies of a line (x axis, where lines are rows and the transform
+// index is the contiguous one); otherwise consecutive threads take consecutive lines.
+
+template <typename C, int R1, bool BFAST>
+__global__ void __launch_bounds__(kThreads) axis_kernel(AxisArgs<C> a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *sm = reinterpret_cast<C *>(smem_raw);
+    const AxisPlan &p = a.plan;
+    const TileGeom &g = a.g;
+    const int n = p.n, q = n / R1, NL = g.nlines, LS = g.LS;
+    int fslot[3], fid[3], nf = 0;
+    for (int f = 0; f < 3; f++)
+        if (a.tmask & (1u << f)) { fslot[nf] = nf; fid[nf] = f; nf++; }
+    const int items = q * NL * nf;
+
+    for (int tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
+        const long long base = tile_base(g, tile);
+        for (int w = threadIdx.x; w < items; w += blockDim.x) {
+            int f, b, l;
+            if (BFAST) {
+                b = w % q;
+                const int r = w / q;
+                l = r % NL;
+                f = r / NL;
+            } else {
+                l = w % NL;
+                const int r = w / NL;
+                b = r % q;
+                f = r / q;
+            }
+            const C *src = a.f[fid[f]] + base + (long long)l * g.gs_l + (long long)b * g.gs_j;
+            C x[R1];
+#pragma unroll
+            for (int m = 0; m < R1; m++) x[m] = src[(long long)m * q * g.gs_j];
+            dft<R1, -1>(x);
+#pragma unroll
+            for (int k = 1; k < R1; k++) x[k] = twmul<-1>(x[k], __ldg(a.tw + (k - 1) * q + b));
+            C *s = sm + (size_t)fslot[f] * n * LS + l;
+#pragma unroll
+            for (int k = 0; k < R1; k++) s[(b + k * q) * LS] = x[k];
+        }
+        __syncthreads();
+        middle_stages<C, -1>(sm, g, p, a.tw, a.tab, nf, fslot, fid);
+        for (int w = threadIdx.x; w < items; w += blockDim.x) {
+            int f, b, l;
+            if (BFAST) {
+                b = w % q;
+                const int r = w / q;
+                l = r % NL;
+                f = r / NL;
+            } else {
+                l = w % NL;
+                const int r = w / NL;
+                b = r % q;
+                f = r / q;
+            }
+            C *s = sm + (size_t)fslot[f] * n * LS + l;
+            C x[R1];
+#pragma unroll
+            for (int m = 0; m < R1; m++) x[m] = s[(b + m * q) * LS];
+#pragma unroll
+            for (int m = 1; m < R1; m++) x[m] = twmul<+1>(x[m], __ldg(a.tw + (m - 1) * q + b));
+            dft<R1, +1>(x);
+            C *dst = a.f[fid[f]] + base + (long long)l * g.gs_l + (long long)b * g.gs_j;
+#pragma unroll
+            for (int k = 0; k < R1; k++) dst[(long long)k * q * g.gs_j] = x[k];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// FP64 sums of |A|^2 for three fields: per-block partials, then one block adds the
+// partials in a fixed order (deterministic).
+
+template <typename C>
+__global__ void __launch_bounds__(kThreads) sums_partial_kernel(const C *f0, const C *f1, const C *f2,
+                                                                 size_t n, double *partials)
+{
+    __shared__ double red[3][kThreads / 32];
+    double acc[3] = {0, 0, 0};
+    const C *fs[3] = {f0, f1, f2};
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (size_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            C a = fs[k][v];
+            acc[k] += (double)a.x * (double)a.x + (double)a.y * (double)a.y;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        double v = acc[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double v = 0;
+        for (int wv = 0; wv < kThreads / 32; wv++) v += red[threadIdx.x][wv];
+        partials[(size_t)blockIdx.x * 3 + threadIdx.x] = v;
+    }
+}
+
+__global__ void sums_final_kernel(const double *partials, int nblocks, double *out)
+{
+    if (threadIdx.x < 3) {
+        double v = 0;
+        for (int b = 0; b < nblocks; b++) v += partials[(size_t)b * 3 + threadIdx.x];
+        out[threadIdx.x] = v;
+    }
+}
+
+__global__ void convert_d2f_kernel(const double2 *src, float2 *dst, size_t n)
+{
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (size_t)gridDim.x * blockDim.x)
+        dst[v] = make_float2((float)src[v].x, (float)src[v].y);
+}
+
+__global__ void convert_f2d_kernel(const float2 *src, double2 *dst, size_t n)
+{
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (size_t)gridDim.x * blockDim.x)
+        dst[v] = make_double2(src[v].x, src[v].y);
+}
+
+// ---------------------------------------------------------------------------------
+// Launchers.
+
+template <typename C, int R1> static cudaError_t set_attr_t(size_t smem)
+{
+    return cudaFuncSetAttribute(tpass_kernel<C, R1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+template <typename C, int R1, bool B> static cudaError_t set_attr_a(size_t smem)
+{
+    return cudaFuncSetAttribute(axis_kernel<C, R1, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+cudaError_t configure_kernels(size_t smem)
+{
+    cudaError_t e = cudaSuccess;
+#define OPO_ATTR(expr) \
+    if ((e = (expr)) != cudaSuccess) return e;
+    OPO_ATTR((set_attr_t<float2, 4>(smem)));
+    OPO_ATTR((set_attr_t<float2, 8>(smem)));
+    OPO_ATTR((set_attr_t<float2, 16>(smem)));
+    OPO_ATTR((set_attr_t<double2, 4>(smem)));
+    OPO_ATTR((set_attr_t<double2, 8>(smem)));
+    OPO_ATTR((set_attr_a<float2, 4, true>(smem)));
+    OPO_ATTR((set_attr_a<float2, 8, true>(smem)));
+    OPO_ATTR((set_attr_a<float2, 16, true>(smem)));
+    OPO_ATTR((set_attr_a<float2, 4, false>(smem)));
+    OPO_ATTR((set_attr_a<float2, 8, false>(smem)));
+    OPO_ATTR((set_attr_a<float2, 16, false>(smem)));
+    OPO_ATTR((set_attr_a<double2, 4, true>(smem)));
+    OPO_ATTR((set_attr_a<double2, 8, true>(smem)));
+    OPO_ATTR((set_attr_a<double2, 16, true>(smem)));
+    OPO_ATTR((set_attr_a<double2, 4, false>(smem)));
+    OPO_ATTR((set_attr_a<double2, 8, false>(smem)));
+    OPO_ATTR((set_attr_a<double2, 16, false>(smem)));
+#undef OPO_ATTR
+    return e;
+}
+
+template <typename C>
+cudaError_t launch_tpass(const TPassArgs<C> &a, int r1, int grid, size_t smem, cudaStream_t st)
+{
+    switch (r1) {
+    case 4: tpass_kernel<C, 4><<<grid, kThreads, smem, st>>>(a); break;
+    case 8: tpass_kernel<C, 8><<<grid, kThreads, smem, st>>>(a); break;
+    case 16:
+        if constexpr (sizeof(C) == 8) {
+            tpass_kernel<C, 16><<<grid, kThreads, smem, st>>>(a);
+            break;
+        }
+        return cudaErrorInvalidValue;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <typename C>
+cudaError_t launch_axis(const AxisArgs<C> &a, int r1, bool bfast, int grid, size_t smem, cudaStream_t st)
+{
+#define OPO_AX(R)                                                           \
+    case R:                                                                 \
+        if (bfast) axis_kernel<C, R, true><<<grid, kThreads, smem, st>>>(a);  \
+        else axis_kernel<C, R, false><<<grid, kThreads, smem, st>>>(a);       \
+        break;
+    switch (r1) {
+        OPO_AX(4)
+        OPO_AX(8)
+        OPO_AX(16)
+    default: return cudaErrorInvalidValue;
+    }
+#undef OPO_AX
+    return cudaGetLastError();
+}
+
+template <typename C>
+cudaError_t launch_sums(const C *f0, const C *f1, const C *f2, size_t n, double *partials, int nblocks,
+                        double *out, cudaStream_t st)
+{
+    sums_partial_kernel<C><<<nblocks, kThreads, 0, st>>>(f0, f1, f2, n, partials);
+    sums_final_kernel<<<1, 32, 0, st>>>(partials, nblocks, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_convert_d2f(const double2 *src, float2 *dst, size_t n, cudaStream_t st)
+{
+    int blocks = (int)((n + kThreads - 1) / kThreads);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    convert_d2f_kernel<<<blocks, kThreads, 0, st>>>(src, dst, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_convert_f2d(const float2 *src, double2 *dst, size_t n, cudaStream_t st)
+{
+    int blocks = (int)((n + kThreads - 1) / kThreads);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    convert_f2d_kernel<<<blocks, kThreads, 0, st>>>(src, dst, n);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_tpass<float2>(const TPassArgs<float2> &, int, int, size_t, cudaStream_t);
+template cudaError_t launch_tpass<double2>(const TPassArgs<double2> &, int, int, size_t, cudaStream_t);
+template cudaError_t launch_axis<float2>(const AxisArgs<float2> &, int, bool, int, size_t, cudaStream_t);
+template cudaError_t launch_axis<double2>(const AxisArgs<double2> &, int, bool, int, size_t, cudaStream_t);
+template cudaError_t launch_sums<float2>(const float2 *, const float2 *, const float2 *, size_t, double *, int,
+                                         double *, cudaStream_t);
+template cudaError_t launch_sums<double2>(const double2 *, const double2 *, const double2 *, size_t, double *,
+                                          int, double *, cudaStream_t);
+
+}  // namespace opo

@@ -1,0 +1,182 @@
+/* cuopo3d.h -- C-ABI of the B200-native split-step Fourier solver for three coupled
+ * chi(2) fields (pump, signal, idler) in an optical parametric oscillator.
+ *
+ * This is the boundary a caller binds (C, C++, ctypes, cgo ...): plain pointers,
+ * sizes and int status codes; no CUDA or torch types.  It replaces the C++ template
+ * interface of alfredos84/cuOPO3D (src/headers), whose classes keep working through
+ * the drop-in headers in src/headers of this repository.  Each entry point names the
+ * reference interface it stands in for (file:line, paths in that project).
+ *
+ * Layout: every field is a complex array in the reference order [t][y][x], x fastest
+ * (reference src/headers/Common.cuh:167-170).  Host-side complex values are
+ * interleaved (re, im) doubles (OPO_FP64) or floats (OPO_FP32).
+ *
+ * Threading: one host thread per solver; solvers are independent; calls on one
+ * solver are ordered on its CUDA stream.  Errors never exit the process: every call
+ * returns an OPO_* status and opo_last_error() explains the last failure.
+ */
+#ifndef CUOPO3D_H
+#define CUOPO3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------ */
+enum {
+    OPO_OK = 0,
+    OPO_ERR_INVALID = 1,     /* bad argument or unsupported size                      */
+    OPO_ERR_CUDA = 2,        /* a CUDA runtime call failed                            */
+    OPO_ERR_NOMEM = 3,       /* device allocation failed                              */
+    OPO_ERR_NONFINITE = 4,   /* a field became NaN/Inf (reference Solver3D.cuh:999-1005) */
+    OPO_ERR_COURANT = 5,     /* reference step-size gate failed (Solver3D.cuh:973,1016-1019) */
+    OPO_ERR_CAPACITY = 6     /* request exceeds a fixed capacity                      */
+};
+
+/* ---- semantics flags (OpoConfig.flags / OpoParams.flags) ----------------------- */
+enum {
+    OPO_DISPERSION = 1u << 0,  /* t-axis step: reference -DDISPERSION (cuOPO3D.sh:38)   */
+    OPO_DIFFRACTION = 1u << 1, /* (x,y) step: reference -DDIFFRACTION (cuOPO3D.sh:38)   */
+    OPO_PHYSICS = 1u << 2,     /* corrected physics: RK4 stages with h, exp(i dk z),
+                                  absorption once, kp/ki from their own indices       */
+    OPO_ASIS_Q1 = 1u << 3,     /* shipped diffraction scale 1/(NX NY NT)
+                                  (Solver3D.cuh:83,780)                                 */
+    OPO_ASIS_Q2 = 1u << 4      /* shipped dispersion on row y=0 only, scale 1/(NX NY NT)
+                                  (Solver3D.cuh:603,613,616,629)                        */
+};
+
+enum { OPO_FP32 = 0, OPO_FP64 = 1 };                  /* bulk field precision          */
+enum { OPO_PPLN = 0, OPO_MGOSPPLT = 1 };               /* crystal models                */
+enum {                                                 /* pump profiles                 */
+    OPO_PUMP_WAVEPLANE_CW = 0,     /* EFields3D.cuh:72-85    */
+    OPO_PUMP_WAVEPLANE_PULSED = 1, /* EFields3D.cuh:89-103   */
+    OPO_PUMP_FOCUSED_CW = 2,       /* EFields3D.cuh:107-120  */
+    OPO_PUMP_FOCUSED_PULSED = 3,   /* EFields3D.cuh:124-137  */
+    OPO_PUMP_FOCUSED_SECH2 = 4,    /* new: sech^2 intensity, P = window-average power */
+    OPO_PUMP_WAVEPLANE_SECH2 = 5   /* new */
+};
+enum {                                                 /* field selectors               */
+    OPO_FIELD_PUMP_INITIAL = 0,    /* EFields::Api */
+    OPO_FIELD_PUMP = 1,            /* EFields::Ap  */
+    OPO_FIELD_SIGNAL = 2,          /* EFields::As  */
+    OPO_FIELD_IDLER = 3            /* EFields::Ai  */
+};
+enum { OPO_MEM_HOST = 0, OPO_MEM_DEVICE = 1 };
+
+/* ---- physical description (the knobs of the reference main(), cuOPO3D.cu:15-51) --- */
+typedef struct OpoConfig {
+    int crystal;                       /* OPO_PPLN / OPO_MGOSPPLT                         */
+    double LX, LY, Lcr, T, Lambda;     /* um, um, um, degC, um                            */
+    double lp, ls;                     /* pump, signal wavelength (um); li = ls lp/(ls-lp) */
+    int nx, ny, nt, nz;                /* grid; nz slices, dz = Lcr/(nz-1)                */
+    double dQ;                         /* um/V; <= 0 keeps the crystal's 2 d33/pi          */
+    double alpha[3];                   /* 1/um; < 0 keeps the crystal's value              */
+    double Lcav, Rs, Ri;               /* cavity length (um); mirror reflectivities        */
+    double gdd_gamma;                  /* GDD compensation fraction, 0 = off               */
+    double detuning;                   /* round-trip phase at the mirrors (rad)            */
+    double P, FWHM, w0, focal;         /* W, ps, um, um                                     */
+    int pump_mode;                     /* OPO_PUMP_*                                        */
+    double t_window;                   /* ps; <= 0: the cavity round-trip time             */
+    unsigned flags;                    /* OPO_DISPERSION | OPO_DIFFRACTION | ...           */
+    int zloop_f32;                     /* step count from the shipped FP32 z loop (1) or FP64 (0) */
+    int n_steps;                       /* > 0: explicit z-step count (dz = Lcr/n_steps in physics mode) */
+    int total_rt;                      /* round trips of the run (the last skips free space) */
+    int precision;                     /* OPO_FP32 / OPO_FP64                               */
+    unsigned resonant;                 /* bit1 signal, bit2 idler (reference resFields)     */
+} OpoConfig;
+
+/* ---- derived solver parameters (what the split-step consumes) ------------------- */
+typedef struct OpoParams {
+    int nx, ny, nt, n_steps;
+    unsigned flags;
+    int precision;
+    double dz, Lcr, dx, dy;
+    double kappa[3];   /* coupling, EFields3D.cuh:219-221                               */
+    double kdiff[3];   /* wavevectors of the diffraction propagator, EFields3D.cuh:222-224 */
+    double vinv[3];    /* group delay relative to the frame, Solver3D.cuh:163-165         */
+    double beta2[3];
+    double alpha[3];
+    double dk;
+    double Rs, Ri, detuning, gdd, free_len;
+    unsigned resonant;
+    int total_rt;
+    double t_window;
+} OpoParams;
+
+/* Derived scalars written by opo_params_from_config (reference names, in order):
+ * np ns ni vp vs vi b2p b2s b2i b3p b3s b3i dQ dk dx dy dz kp ks ki
+ * kappa_p kappa_s kappa_i trt dt nsteps */
+#define OPO_N_SCALARS 26
+
+typedef struct OpoSolver OpoSolver;
+
+/* ---- host physics (the reference's constructors) --------------------------------- */
+
+/* Crystal, EFields and Cavity constructors in one: Sellmeier indices, group
+ * velocities, GVD, TOD, kappa, k, dk, steps, round-trip time and the z-step count.
+ * Replaces PPLN::PPLN (CrystalsBase/PPLN.cuh:51-78), MgOsPPLT::MgOsPPLT
+ * (CrystalsBase/MgOsPPLT.cuh:51-78), EFields::EFields (EFields3D.cuh:199-227) and
+ * Cavity::Cavity (Cavity3D.cuh:42-49).  scalars may be NULL. */
+int opo_params_from_config(const OpoConfig *cfg, OpoParams *out, double *scalars);
+
+/* Refractive index n, group velocity, GVD and TOD of a crystal at one wavelength
+ * (PPLN.cuh:97-259, MgOsPPLT.cuh:96-226).  out = {n, vg, b2, b3}. */
+int opo_crystal_dispersion(int crystal, double T, double lambda_um, double out[4]);
+
+/* Time and angular-frequency grids, EFields::setTimeFreqVectors
+ * (EFields3D.cuh:319-328): t = linspace(-T/2, T/2), w = 2 pi fftshift(linspace(
+ * -nt/(2T), nt/(2T))).  Either pointer may be NULL. */
+int opo_time_freq(int nt, double window, double *t, double *w);
+
+/* Initial pump field, EFields::setPumpField (EFields3D.cuh:244-296), into
+ * Api (interleaved complex128, nx*ny*nt values). */
+int opo_pump_field(const OpoConfig *cfg, double *Api);
+
+/* Seeded noise replacing EFields::noiseGenerator (EFields3D.cuh:300-315): each
+ * component is sigma (sum of 12 splitmix64 uniforms - 6); deterministic everywhere. */
+int opo_noise(uint64_t seed, double sigma, size_t n_complex, double *out);
+
+/* ---- solver ------------------------------------------------------------------------ */
+
+/* Allocate the resident fields, phase tables and FFT plans on the current device.
+ * w: nt angular frequencies (host doubles, opo_time_freq).  Replaces
+ * Solver::Solver (Solver3D.cuh:456-468) plus setDispersionPropagators (:550-567)
+ * and setDiffractionPropagators (:700-721), which are built once here. */
+int opo_create(const OpoParams *p, const double *w, OpoSolver **out);
+void opo_destroy(OpoSolver *s);
+
+/* Copy a field in or out.  where = OPO_MEM_HOST / OPO_MEM_DEVICE; elem_precision
+ * is the caller buffer's precision (converted on the device if it differs).
+ * Stands in for the thrust assignments on EFields::Api/Ap/As/Ai
+ * (cuOPO3D.cu:46,51; Solver3D.cuh:981). */
+int opo_set_field(OpoSolver *s, int which, const void *src, int where, int elem_precision);
+int opo_get_field(OpoSolver *s, int which, void *dst, int where, int elem_precision);
+
+/* One pass through the crystal without cavity, Solver::runSinglePass
+ * (Solver3D.cuh:1031-1043; SSFM :946-960). */
+int opo_run_single_pass(OpoSolver *s);
+
+/* n cavity round trips continuing from the solver's round-trip counter,
+ * Solver::runOPO (Solver3D.cuh:964-1023): fresh pump, SSFM, free-space return
+ * (skipped on round trip total_rt-1), GDD compensation, mirrors. */
+int opo_run_round_trips(OpoSolver *s, int n);
+
+/* FP64 sum of |A|^2 over every voxel of the pump, signal and idler (in that order);
+ * the reference's averagePowerCutXY (Solver3D.cuh:529-545) is
+ * 0.5 eps0 c ns dx dy / (LX LY) times the signal entry. */
+int opo_field_sums(OpoSolver *s, double sums[3]);
+
+int opo_synchronize(OpoSolver *s);
+int opo_round_trip_index(const OpoSolver *s);
+/* Number of kernels this solver has launched since creation (graph nodes included). */
+long long opo_kernel_launches(const OpoSolver *s);
+const char *opo_last_error(const OpoSolver *s);
+const char *opo_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUOPO3D_H */
