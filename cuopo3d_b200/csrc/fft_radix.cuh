@@ -13,25 +13,25 @@ template <typename T> struct Cpx;
 template <> struct Cpx<float> { using type = float2; };
 template <> struct Cpx<double> { using type = double2; };
 
-template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return C{a.x + b.x, a.y + b.y}; }
-template <typename C> __device__ __forceinline__ C csub(C a, C b) { return C{a.x - b.x, a.y - b.y}; }
-template <typename C> __device__ __forceinline__ C cmul(C a, C b)
+template <typename C> __host__ __device__ __forceinline__ C cadd(C a, C b) { return C{a.x + b.x, a.y + b.y}; }
+template <typename C> __host__ __device__ __forceinline__ C csub(C a, C b) { return C{a.x - b.x, a.y - b.y}; }
+template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b)
 {
     return C{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
 }
 // a * conj(b)
-template <typename C> __device__ __forceinline__ C cmulc(C a, C b)
+template <typename C> __host__ __device__ __forceinline__ C cmulc(C a, C b)
 {
     return C{a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y};
 }
-template <typename C, typename T> __device__ __forceinline__ C cscale(C a, T s) { return C{a.x * s, a.y * s}; }
+template <typename C, typename T> __host__ __device__ __forceinline__ C cscale(C a, T s) { return C{a.x * s, a.y * s}; }
 // a * (S i)
-template <int S, typename C> __device__ __forceinline__ C cmul_si(C a)
+template <int S, typename C> __host__ __device__ __forceinline__ C cmul_si(C a)
 {
     return S > 0 ? C{-a.y, a.x} : C{a.y, -a.x};
 }
 // a * (c + S i s) for real c, s
-template <int S, typename C, typename T> __device__ __forceinline__ C cmul_cs(C a, T c, T s)
+template <int S, typename C, typename T> __host__ __device__ __forceinline__ C cmul_cs(C a, T c, T s)
 {
     return S > 0 ? C{a.x * c - a.y * s, a.x * s + a.y * c} : C{a.x * c + a.y * s, a.y * c - a.x * s};
 }
@@ -44,14 +44,14 @@ template <typename T> struct Roots {
     static constexpr T s3 = T(0.86602540378443864676);  // sin(pi/3)
 };
 
-template <int S, typename C> __device__ __forceinline__ void dft2(C &a, C &b)
+template <int S, typename C> __host__ __device__ __forceinline__ void dft2(C &a, C &b)
 {
     C t = a;
     a = cadd(t, b);
     b = csub(t, b);
 }
 
-template <int S, typename C> __device__ __forceinline__ void dft4(C &x0, C &x1, C &x2, C &x3)
+template <int S, typename C> __host__ __device__ __forceinline__ void dft4(C &x0, C &x1, C &x2, C &x3)
 {
     C t0 = cadd(x0, x2), t1 = csub(x0, x2);
     C t2 = cadd(x1, x3), t3 = cmul_si<S>(csub(x1, x3));
@@ -64,11 +64,11 @@ template <int S, typename C> __device__ __forceinline__ void dft4(C &x0, C &x1, 
 template <int R, int S, typename C> struct Dft;
 
 template <int S, typename C> struct Dft<2, S, C> {
-    __device__ __forceinline__ static void run(C *x) { dft2<S>(x[0], x[1]); }
+    __host__ __device__ __forceinline__ static void run(C *x) { dft2<S>(x[0], x[1]); }
 };
 
 template <int S, typename C> struct Dft<3, S, C> {
-    __device__ __forceinline__ static void run(C *x)
+    __host__ __device__ __forceinline__ static void run(C *x)
     {
         using T = decltype(x[0].x);
         C t1 = cadd(x[1], x[2]);
@@ -81,12 +81,12 @@ template <int S, typename C> struct Dft<3, S, C> {
 };
 
 template <int S, typename C> struct Dft<4, S, C> {
-    __device__ __forceinline__ static void run(C *x) { dft4<S>(x[0], x[1], x[2], x[3]); }
+    __host__ __device__ __forceinline__ static void run(C *x) { dft4<S>(x[0], x[1], x[2], x[3]); }
 };
 
 // 8 = 2 x 4: a_m = x_m + x_{m+4}, b_m = (x_m - x_{m+4}) W8^m, y_{2k} = DFT4(a), y_{2k+1} = DFT4(b)
 template <int S, typename C> struct Dft<8, S, C> {
-    __device__ __forceinline__ static void run(C *x)
+    __host__ __device__ __forceinline__ static void run(C *x)
     {
         using T = decltype(x[0].x);
         const T r2 = Roots<T>::r2;
@@ -104,7 +104,7 @@ template <int S, typename C> struct Dft<8, S, C> {
 
 // 16 = 4 x 4: u_{m,r} = DFT4_j(x_{m+4j})_r, u_{m,r} *= W16^{m r}, y_{4k+r} = DFT4_m(u_{m,r})_k
 template <int S, typename C> struct Dft<16, S, C> {
-    __device__ __forceinline__ static void run(C *x)
+    __host__ __device__ __forceinline__ static void run(C *x)
     {
         using T = decltype(x[0].x);
         const T r2 = Roots<T>::r2, c8 = Roots<T>::c8, s8 = Roots<T>::s8;
@@ -133,6 +133,6 @@ template <int S, typename C> struct Dft<16, S, C> {
     }
 };
 
-template <int R, int S, typename C> __device__ __forceinline__ void dft(C *x) { Dft<R, S, C>::run(x); }
+template <int R, int S, typename C> __host__ __device__ __forceinline__ void dft(C *x) { Dft<R, S, C>::run(x); }
 
 }  // namespace opo

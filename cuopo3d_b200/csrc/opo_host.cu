@@ -771,7 +771,9 @@ int opo_create(const OpoParams *p, const double *w, OpoSolver **out)
         if (s->smem_x > mx) mx = s->smem_x;
         if (s->smem_y > mx) mx = s->smem_y;
         if (mx > 227 * 1024) { rc = fail(s, OPO_ERR_INVALID, "tile does not fit in shared memory"); break; }
-        if ((e = opo::configure_kernels(96 * 1024 > mx ? 96 * 1024 : mx)) != cudaSuccess) {
+        // The attribute is per kernel function and shared by every solver of the process:
+        // always allow the full 227 KB so no solver lowers it under another.
+        if ((e = opo::configure_kernels(227 * 1024)) != cudaSuccess) {
             rc = cuda_fail(s, e, "configure kernels");
             break;
         }

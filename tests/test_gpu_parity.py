@@ -1,0 +1,233 @@
+"""Parity of the CUDA path (libcuopo3d.so through the C-ABI) against the reference's
+own outputs (tests/golden) and against the FP64 CPU oracle.
+
+Tolerances (relative L2 field error): FP64 plain form <= 1e-10 against the FP64
+reference build and the oracle; FP32 precision form <= 1e-5 against FP64; the
+as-shipped FP32 reference (quirks Q1/Q2) <= 5e-4 (its own FP32 rounding)."""
+import numpy as np
+import pytest
+
+import cuopo3d_b200 as co
+from golden_cases import Golden, fixture_names, rel_l2
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+FP32_TOL = 1e-5
+
+
+def run_lib(cfg, s0, i0, mode, nrt=1, api=None):
+    params, _ = co.derive(cfg)
+    _, w = co.time_freq(cfg.nt, params.t_window)
+    sim = co.Simulation(params, w)
+    if api is None:
+        api = co.pump_field(cfg)
+    sim.set_field(co.FIELD_API, api)
+    sim.set_field(co.FIELD_AP, api)
+    sim.set_field(co.FIELD_AS, s0)
+    sim.set_field(co.FIELD_AI, i0)
+    if mode == "single":
+        sim.run_single_pass()
+    else:
+        sim.run_round_trips(nrt)
+    out = (sim.get_field(co.FIELD_AP), sim.get_field(co.FIELD_AS), sim.get_field(co.FIELD_AI))
+    return sim, out
+
+
+def run_oracle(kw, flags, s0, i0, mode, nrt=1):
+    st = po.Setup(po.make_phys(flags=flags, **kw))
+    api = st.api_complex()
+    if mode == "single":
+        return po.single_pass(st, api, s0, i0)
+    return po.round_trips(st, api, api, s0, i0, nrt)
+
+
+def assert_close(out, ref, tol, tidx=None):
+    for a, b, name in zip(out, ref, ("Ap", "As", "Ai")):
+        a = a if tidx is None else a[tidx]
+        e = rel_l2(a, b)
+        assert e < tol, (name, e)
+
+
+FP64_FIXTURES = [n for n in fixture_names() if Golden(n).fp64]
+
+
+@pytest.mark.parametrize("name", FP64_FIXTURES)
+def test_fp64_matches_reference(name):
+    """Plain FP64 form against the FP64 reference build (its own cuFFT pipeline)."""
+    g = Golden(name)
+    cfg = co.make_config(precision=co.FP64, **g.config_kwargs())
+    s0, i0 = g.initial_fields(co.noise)
+    _, out = run_lib(cfg, s0, i0, g.mode, g.nrt)
+    assert_close(out, (g.Ap, g.As, g.Ai), FP64_TOL, g.tidx)
+
+
+def test_asis_fp32_reference_quirks():
+    """Shipped quirks Q1 (diffraction scale 1/SIZE) and Q2 (dispersion on row y=0 only)."""
+    g = Golden("g16_asis_fp32")
+    cfg = co.make_config(precision=co.FP64, flags=co.DISPERSION | co.DIFFRACTION | co.ASIS_Q1 | co.ASIS_Q2,
+                         **g.config_kwargs())
+    s0, i0 = g.initial_fields(co.noise)
+    _, out = run_lib(cfg, s0, i0, g.mode, g.nrt)
+    assert_close(out, (g.Ap, g.As, g.Ai), 5e-4, g.tidx)
+
+
+@pytest.mark.parametrize("name", fixture_names())
+def test_fp32_precision_form_vs_oracle(name):
+    """FP32 bulk fields with FP64 tables against the FP64 oracle on the same inputs."""
+    g = Golden(name)
+    kw = g.config_kwargs()
+    flags = co.DISPERSION | co.DIFFRACTION | ((co.ASIS_Q1 | co.ASIS_Q2) if g.asis else 0)
+    s0, i0 = g.initial_fields(co.noise)
+    _, out = run_lib(co.make_config(precision=co.FP32, flags=flags, **kw), s0, i0, g.mode, g.nrt)
+    ref = run_oracle(kw, flags, s0, i0, g.mode, g.nrt)
+    tol = FP32_TOL if not g.asis else 1e-4
+    assert_close(out, ref, tol)
+
+
+GRIDS = [(8, 8, 16), (16, 8, 32), (12, 12, 24), (24, 16, 48), (32, 32, 64), (64, 32, 128),
+         (96, 96, 192), (16, 16, 2048), (128, 128, 16)]
+
+
+@pytest.mark.parametrize("nx,ny,nt", GRIDS)
+def test_grid_shapes_fp64_vs_oracle(nx, ny, nt):
+    """Radix-2/3 plans, non-square grids, long and short time axes."""
+    kw = dict(nx=nx, ny=ny, nt=nt, nz=4, LX=300.0, LY=250.0, Lcr=3000.0, P=500.0, w0=40.0, FWHM=3.0,
+              t_window=25.0, pump_mode="focused-pulsed")
+    s0 = co.noise(5, 0.02, nx * ny * nt).reshape(nt, ny, nx)
+    i0 = co.noise(6, 0.02, nx * ny * nt).reshape(nt, ny, nx)
+    flags = co.DISPERSION | co.DIFFRACTION
+    _, out = run_lib(co.make_config(precision=co.FP64, flags=flags, **kw), s0, i0, "single")
+    ref = run_oracle(kw, flags, s0, i0, "single")
+    assert_close(out, ref, FP64_TOL)
+
+
+@pytest.mark.parametrize("flags", [co.DISPERSION | co.DIFFRACTION | co.PHYSICS, co.DIFFRACTION, co.DISPERSION,
+                                   co.DISPERSION | co.DIFFRACTION | co.PHYSICS | co.ASIS_Q1])
+def test_flag_combinations_round_trips(flags):
+    kw = dict(nx=16, ny=16, nt=32, nz=6, LX=300.0, LY=300.0, Lcr=4000.0, Lambda=6.5, P=300.0, w0=40.0,
+              FWHM=4.0, t_window=30.0, pump_mode="focused-pulsed", gdd_gamma=0.7, Rs=0.9, Ri=0.8,
+              detuning=0.3, total_rt=4)
+    s0 = co.noise(9, 0.01, 16 * 16 * 32).reshape(32, 16, 16)
+    i0 = s0.copy()
+    _, out = run_lib(co.make_config(precision=co.FP64, flags=flags, **kw), s0, i0, "opo", 4)
+    ref = run_oracle(kw, flags, s0, i0, "opo", 4)
+    assert_close(out, ref, FP64_TOL)
+
+
+def test_round_trips_resume_and_last_skip():
+    """3 + 2 round trips equal 5 at once; the run's last round trip skips the free-space
+    return (Solver3D.cuh:987) both ways."""
+    kw = dict(nx=16, ny=16, nt=32, nz=5, Lcr=3000.0, P=200.0, w0=40.0, pump_mode="focused-cw",
+              gdd_gamma=1.0, total_rt=5)
+    s0 = co.noise(3, 0.01, 16 * 16 * 32).reshape(32, 16, 16)
+    cfg = co.make_config(precision=co.FP64, **kw)
+    sim_a, out_a = run_lib(cfg, s0, s0, "opo", 5)
+    params, _ = co.derive(cfg)
+    _, w = co.time_freq(cfg.nt, params.t_window)
+    sim = co.Simulation(params, w)
+    api = co.pump_field(cfg)
+    for which, arr in ((co.FIELD_API, api), (co.FIELD_AP, api), (co.FIELD_AS, s0), (co.FIELD_AI, s0)):
+        sim.set_field(which, arr)
+    sim.run_round_trips(3)
+    sim.run_round_trips(2)
+    assert sim.round_trip_index == 5
+    out_b = (sim.get_field(co.FIELD_AP), sim.get_field(co.FIELD_AS), sim.get_field(co.FIELD_AI))
+    for a, b in zip(out_a, out_b):
+        assert np.array_equal(a, b)
+    ref = run_oracle(kw, co.DISPERSION | co.DIFFRACTION, s0, s0, "opo", 5)
+    assert_close(out_a, ref, FP64_TOL)
+
+
+def test_field_sums_and_launch_count():
+    kw = dict(nx=32, ny=16, nt=64, nz=5, P=100.0, pump_mode="focused-pulsed", t_window=20.0)
+    cfg = co.make_config(precision=co.FP32, **kw)
+    s0 = co.noise(1, 0.01, 32 * 16 * 64).reshape(64, 16, 32)
+    sim, out = run_lib(cfg, s0, s0 * 0.5, "opo", 2)
+    sums = sim.field_sums()
+    for k in range(3):
+        ref = float(np.sum(np.abs(out[k]) ** 2))
+        assert abs(sums[k] - ref) <= 1e-6 * ref
+    params, _ = co.derive(cfg)
+    n = params.n_steps
+    # per round trip: n t-passes, n x- and y-passes, the closing t-pass, the free-space x/y
+    assert sim.kernel_launches >= 2 * (3 * n + 1) + 2
+
+
+def test_nonfinite_field_is_reported():
+    """A NaN in the fields yields an error status from the FP64 tallies, not a fault."""
+    kw = dict(nx=8, ny=8, nt=16, nz=4)
+    cfg = co.make_config(precision=co.FP64, **kw)
+    s0 = np.zeros((16, 8, 8), np.complex128)
+    s0[3, 2, 1] = np.nan
+    sim, _ = run_lib(cfg, s0, s0, "single")
+    with pytest.raises(co.OpoError) as e:
+        sim.field_sums()
+    assert e.value.code == co.OPO_ERR_NONFINITE
+
+
+def test_device_pointer_field_io():
+    torch = pytest.importorskip("torch")
+    kw = dict(nx=16, ny=8, nt=32, nz=4)
+    cfg = co.make_config(precision=co.FP32, **kw)
+    params, _ = co.derive(cfg)
+    _, w = co.time_freq(cfg.nt, params.t_window)
+    sim = co.Simulation(params, w)
+    x = co.noise(4, 1.0, 16 * 8 * 32)
+    d64 = torch.from_numpy(x.copy()).cuda()
+    sim.set_field_device(co.FIELD_AS, d64.data_ptr(), co.FP64)
+    d32 = torch.empty(x.size, dtype=torch.complex64, device="cuda")
+    sim.get_field_device(co.FIELD_AS, d32.data_ptr(), co.FP32)
+    sim.synchronize()
+    assert np.allclose(d32.cpu().numpy(), x.astype(np.complex64), rtol=0, atol=1e-6)
+    host = sim.get_field(co.FIELD_AS)
+    assert np.allclose(host.ravel(), x, rtol=1e-6, atol=1e-7)
+
+
+def test_full_size_energy_conservation_linear():
+    """C2 grid (128^2 x 256), FP64: without coupling or absorption the split-step is
+    unitary per field, so every field's sum |A|^2 is conserved."""
+    kw = dict(nx=128, ny=128, nt=256, nz=10, LX=800.0, LY=800.0, Lcr=20000.0, t_window=40.0, P=5.0,
+              w0=60.0, FWHM=2.0, dQ=1e-30, alpha=(0.0, 0.0, 0.0), pump_mode="focused-pulsed")
+    cfg = co.make_config(precision=co.FP64, **kw)
+    V = 128 * 128 * 256
+    s0 = co.noise(2, 1e-3, V).reshape(256, 128, 128)
+    sim, _ = run_lib(cfg, s0, s0 * 0.3, "single")
+    sums = sim.field_sums()
+    api = co.pump_field(cfg)
+    ref = [np.sum(np.abs(api) ** 2), np.sum(np.abs(s0) ** 2), np.sum(np.abs(0.3 * s0) ** 2)]
+    for k in range(3):
+        assert abs(sums[k] / ref[k] - 1) < 1e-11
+
+
+def test_full_size_manley_rowe_physics():
+    """C2 grid, corrected physics, no absorption: sum(|Ap|^2/kp + |As|^2/ks) is conserved
+    by the coupled-wave equations and by the unitary linear steps."""
+    kw = dict(nx=128, ny=128, nt=256, nz=21, LX=800.0, LY=800.0, Lcr=20000.0, t_window=40.0, P=20.0,
+              w0=60.0, FWHM=6.0, alpha=(0.0, 0.0, 0.0), pump_mode="focused-pulsed", n_steps=20)
+    cfg = co.make_config(precision=co.FP64, flags=co.DISPERSION | co.DIFFRACTION | co.PHYSICS, **kw)
+    params, _ = co.derive(cfg)
+    V = 128 * 128 * 256
+    s0 = co.noise(8, 0.05, V).reshape(256, 128, 128)
+    api = co.pump_field(cfg)
+    k = params.kappa
+    before = np.sum(np.abs(api) ** 2) / k[0] + np.sum(np.abs(s0) ** 2) / k[1]
+    sim, out = run_lib(cfg, s0, s0 * 0, "single")
+    s = sim.field_sums()
+    after = s[0] / k[0] + s[1] / k[1]
+    assert abs(s[1] / np.sum(np.abs(s0) ** 2) - 1) > 1e-4  # the signal did exchange energy
+    assert abs(after / before - 1) < 1e-7
+
+
+def test_full_size_fp32_vs_fp64_round_trip():
+    """C2 configuration: one round trip in the FP32 precision form against FP64."""
+    kw = dict(nx=128, ny=128, nt=256, nz=100, LX=800.0, LY=800.0, Lcr=20000.0, t_window=40.0, P=5.0,
+              w0=60.0, FWHM=2.0, Rs=0.98, alpha=(-1.0, 2e-7, 2e-7), pump_mode="focused-pulsed",
+              gdd_gamma=1.0, total_rt=200)
+    V = 128 * 128 * 256
+    s0 = co.noise(1, 1e-3, V).reshape(256, 128, 128)
+    _, o64 = run_lib(co.make_config(precision=co.FP64, **kw), s0, s0, "opo", 1)
+    _, o32 = run_lib(co.make_config(precision=co.FP32, **kw), s0, s0, "opo", 1)
+    for a, b in zip(o32, o64):
+        assert rel_l2(a, b) < FP32_TOL
