@@ -85,6 +85,8 @@ def lib():
         L.opo_run_round_trips.argtypes = [vp, _i]
         L.opo_field_sums.argtypes = [vp, dp]
         L.opo_synchronize.argtypes = [vp]
+        L.opo_set_pass_timing.argtypes = [vp, _i]
+        L.opo_pass_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong)]
         L.opo_round_trip_index.argtypes = [vp]
         L.opo_kernel_launches.argtypes = [vp]
         L.opo_kernel_launches.restype = ctypes.c_longlong
@@ -202,6 +204,16 @@ class Simulation:
         s = np.zeros(3)
         self._check(lib().opo_field_sums(self._h, _dptr(s)))
         return s
+
+    def set_pass_timing(self, enable):
+        self._check(lib().opo_set_pass_timing(self._h, 1 if enable else 0))
+
+    def pass_times(self):
+        """{kind: (total_ms, launches)} for t/x/y passes and other kernels since the last call."""
+        ms = np.zeros(4)
+        cnt = (ctypes.c_longlong * 4)()
+        self._check(lib().opo_pass_times(self._h, _dptr(ms), cnt))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(("t", "x", "y", "other"))}
 
     def synchronize(self):
         self._check(lib().opo_synchronize(self._h))

@@ -230,6 +230,11 @@ struct OpoSolver {
     long long launches = 0;
     int launches_rt[2] = {0, 0};
     bool gdd_or_mirror = false;
+    // per-pass event timing
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    struct Timed { int kind; cudaEvent_t a, b; };
+    std::vector<Timed> timed;
 };
 
 namespace {
@@ -253,6 +258,37 @@ int cuda_fail(OpoSolver *s, cudaError_t e, const char *what)
         cudaError_t e_ = (call);                                \
         if (e_ != cudaSuccess) return cuda_fail((s), e_, what); \
     } while (0)
+
+cudaEvent_t take_event(OpoSolver *s)
+{
+    if (!s->ev_pool.empty()) {
+        cudaEvent_t e = s->ev_pool.back();
+        s->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+
+// Brackets one kernel launch with events when pass timing is on.
+struct PassTimer {
+    OpoSolver *s;
+    int kind;
+    cudaEvent_t a = nullptr;
+    PassTimer(OpoSolver *s_, int k) : s(s_), kind(k)
+    {
+        if (s->timing && (a = take_event(s))) cudaEventRecord(a, s->stream);
+    }
+    ~PassTimer()
+    {
+        if (!a) return;
+        cudaEvent_t b = take_event(s);
+        if (!b) { s->ev_pool.push_back(a); return; }
+        cudaEventRecord(b, s->stream);
+        s->timed.push_back({kind, a, b});
+    }
+};
 
 template <typename C> C to_c(const cd &v);
 template <> float2 to_c<float2>(const cd &v) { return make_float2((float)v.real(), (float)v.imag()); }
@@ -433,6 +469,7 @@ int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, C *con
     a.skip_rows = (p.flags & OPO_ASIS_Q2) ? 1 : 0;
     a.nx = p.nx;
     int grid = a.g.ntiles;
+    PassTimer timer(s, 0);
     OPO_CU(s, opo::launch_tpass<C>(a, s->r1_t, grid, s->smem_t, s->stream), "t-pass launch");
     s->launches++;
     return OPO_OK;
@@ -450,6 +487,7 @@ template <typename C> int enqueue_axis(OpoSolver *s, bool xaxis, C *const *tab, 
     a.tmask = mask;
     const int r1 = xaxis ? s->r1_x : s->r1_y;
     const size_t smem = xaxis ? s->smem_x : s->smem_y;
+    PassTimer timer(s, xaxis ? 1 : 2);
     OPO_CU(s, opo::launch_axis<C>(a, r1, xaxis, a.g.ntiles, smem, s->stream), "axis-pass launch");
     s->launches++;
     return OPO_OK;
@@ -550,6 +588,12 @@ template <typename C> int run_round_trips(OpoSolver *s, int n)
     for (int k = 0; k < n; k++) {
         const bool last = s->rt_index == s->p.total_rt - 1;
         const int gi = last ? 1 : 0;
+        if (s->timing) {
+            int rc = enqueue_round_trip<C>(s, last);
+            if (rc) return rc;
+            s->rt_index++;
+            continue;
+        }
         if (!s->graph_rt[gi]) {
             int rc = build_graph<C>(s, last);
             if (rc) return rc;
@@ -563,9 +607,12 @@ template <typename C> int run_round_trips(OpoSolver *s, int n)
 
 template <typename C> int field_sums(OpoSolver *s, double out[3])
 {
-    OPO_CU(s, opo::launch_sums<C>(fld<C>(s, 1), fld<C>(s, 2), fld<C>(s, 3), s->V, s->partials, s->sum_blocks,
-                                  s->sums_dev, s->stream),
-           "sums launch");
+    {
+        PassTimer timer(s, 3);
+        OPO_CU(s, opo::launch_sums<C>(fld<C>(s, 1), fld<C>(s, 2), fld<C>(s, 3), s->V, s->partials,
+                                      s->sum_blocks, s->sums_dev, s->stream),
+               "sums launch");
+    }
     s->launches += 2;
     OPO_CU(s, cudaMemcpyAsync(out, s->sums_dev, 3 * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "sums copy");
     OPO_CU(s, cudaStreamSynchronize(s->stream), "sums sync");
@@ -800,6 +847,11 @@ void opo_destroy(OpoSolver *s)
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto &g : s->graph_rt)
         if (g) cudaGraphExecDestroy(g);
+    for (auto &t : s->timed) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    for (auto e : s->ev_pool) cudaEventDestroy(e);
     for (auto *pp : s->allocs) cudaFree(pp);
     for (auto *f : s->field)
         if (f) cudaFree(f);
@@ -889,6 +941,31 @@ int opo_synchronize(OpoSolver *s)
 {
     if (!s) return OPO_ERR_INVALID;
     OPO_CU(s, cudaStreamSynchronize(s->stream), "synchronize");
+    return OPO_OK;
+}
+
+int opo_set_pass_timing(OpoSolver *s, int enable)
+{
+    if (!s) return OPO_ERR_INVALID;
+    s->timing = enable != 0;
+    return OPO_OK;
+}
+
+int opo_pass_times(OpoSolver *s, double ms[4], long long counts[4])
+{
+    if (!s || !ms || !counts) return s ? fail(s, OPO_ERR_INVALID, "null output") : OPO_ERR_INVALID;
+    OPO_CU(s, cudaStreamSynchronize(s->stream), "pass-times sync");
+    for (int k = 0; k < 4; k++) { ms[k] = 0; counts[k] = 0; }
+    for (auto &t : s->timed) {
+        float v = 0;
+        if (cudaEventElapsedTime(&v, t.a, t.b) == cudaSuccess) {
+            ms[t.kind] += v;
+            counts[t.kind]++;
+        }
+        s->ev_pool.push_back(t.a);
+        s->ev_pool.push_back(t.b);
+    }
+    s->timed.clear();
     return OPO_OK;
 }
 

@@ -169,6 +169,15 @@ int opo_run_round_trips(OpoSolver *s, int n);
  * 0.5 eps0 c ns dx dy / (LX LY) times the signal entry. */
 int opo_field_sums(OpoSolver *s, double sums[3]);
 
+/* Per-pass device timing with CUDA events on the solver's stream.  While enabled,
+ * passes are launched one by one (round trips are not replayed as graphs) with an event
+ * pair around every pass kernel.  opo_pass_times() waits for the stream, returns the
+ * accumulated milliseconds and launch counts per pass kind since the last call --
+ * [0] t-pass, [1] x-pass, [2] y-pass, [3] other kernels -- and resets them.
+ * No counterpart in the reference (its only timer is the wall clock, Common.cuh:74-90). */
+int opo_set_pass_timing(OpoSolver *s, int enable);
+int opo_pass_times(OpoSolver *s, double ms[4], long long counts[4]);
+
 int opo_synchronize(OpoSolver *s);
 int opo_round_trip_index(const OpoSolver *s);
 /* Number of kernels this solver has launched since creation (graph nodes included). */

@@ -73,17 +73,41 @@ def test_asis_fp32_reference_quirks():
     assert_close(out, (g.Ap, g.As, g.Ai), 5e-4, g.tidx)
 
 
-@pytest.mark.parametrize("name", fixture_names())
-def test_fp32_precision_form_vs_oracle(name):
-    """FP32 bulk fields with FP64 tables against the FP64 oracle on the same inputs."""
+def fp32_vs_oracle(name):
     g = Golden(name)
     kw = g.config_kwargs()
     flags = co.DISPERSION | co.DIFFRACTION | ((co.ASIS_Q1 | co.ASIS_Q2) if g.asis else 0)
     s0, i0 = g.initial_fields(co.noise)
     _, out = run_lib(co.make_config(precision=co.FP32, flags=flags, **kw), s0, i0, g.mode, g.nrt)
     ref = run_oracle(kw, flags, s0, i0, g.mode, g.nrt)
-    tol = FP32_TOL if not g.asis else 1e-4
-    assert_close(out, ref, tol)
+    return g, out, ref
+
+
+@pytest.mark.parametrize("name", [n for n in fixture_names() if Golden(n).mode == "single"])
+def test_fp32_precision_form_single_pass(name):
+    """FP32 bulk fields with FP64 tables against the FP64 oracle, one crystal pass:
+    within the 1e-5 relative field error of the precision form."""
+    g, out, ref = fp32_vs_oracle(name)
+    assert_close(out, ref, FP32_TOL if not g.asis else 1e-4)
+
+
+@pytest.mark.parametrize("name", [n for n in fixture_names() if Golden(n).mode == "opo"])
+def test_fp32_precision_form_round_trips(name):
+    """Ten cavity round trips with parametric gain in FP32: rounding accumulates over
+    ~120 split steps, so the bound is 3e-5 (the shipped FP32 reference build itself is
+    2.9e-5 from the FP64 oracle on g16_opo_fp32)."""
+    _, out, ref = fp32_vs_oracle(name)
+    assert_close(out, ref, 3e-5)
+
+
+def test_fp32_more_accurate_than_reference_fp32():
+    """On the same FP32 round-trip case our FP32 form is closer to the FP64 oracle than
+    the reference's own FP32 cuFFT build."""
+    g, out, ref = fp32_vs_oracle("g16_opo_fp32")
+    for k, name in enumerate(("Ap", "As", "Ai")):
+        ours = rel_l2(out[k][g.tidx], ref[k][g.tidx])
+        theirs = rel_l2(getattr(g, name), ref[k][g.tidx])
+        assert ours <= theirs, (name, ours, theirs)
 
 
 GRIDS = [(8, 8, 16), (16, 8, 32), (12, 12, 24), (24, 16, 48), (32, 32, 64), (64, 32, 128),
