@@ -85,6 +85,7 @@ def lib():
         L.opo_run_round_trips.argtypes = [vp, _i]
         L.opo_field_sums.argtypes = [vp, dp]
         L.opo_synchronize.argtypes = [vp]
+        L.opo_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
         L.opo_set_pass_timing.argtypes = [vp, _i]
         L.opo_pass_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong)]
         L.opo_round_trip_index.argtypes = [vp]
@@ -204,6 +205,13 @@ class Simulation:
         s = np.zeros(3)
         self._check(lib().opo_field_sums(self._h, _dptr(s)))
         return s
+
+    @property
+    def stream(self):
+        """The solver's cudaStream_t as an integer (e.g. for torch.cuda.ExternalStream)."""
+        st = ctypes.c_void_p()
+        self._check(lib().opo_get_stream(self._h, ctypes.byref(st)))
+        return st.value or 0
 
     def set_pass_timing(self, enable):
         self._check(lib().opo_set_pass_timing(self._h, 1 if enable else 0))

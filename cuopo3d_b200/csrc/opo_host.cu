@@ -969,6 +969,13 @@ int opo_pass_times(OpoSolver *s, double ms[4], long long counts[4])
     return OPO_OK;
 }
 
+int opo_get_stream(const OpoSolver *s, void **stream)
+{
+    if (!s || !stream) return OPO_ERR_INVALID;
+    *stream = (void *)s->stream;
+    return OPO_OK;
+}
+
 int opo_round_trip_index(const OpoSolver *s) { return s ? s->rt_index : -1; }
 long long opo_kernel_launches(const OpoSolver *s) { return s ? s->launches : -1; }
 const char *opo_last_error(const OpoSolver *s) { return s ? s->err.c_str() : g_static_err; }

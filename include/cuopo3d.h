@@ -178,6 +178,11 @@ int opo_field_sums(OpoSolver *s, double sums[3]);
 int opo_set_pass_timing(OpoSolver *s, int enable);
 int opo_pass_times(OpoSolver *s, double ms[4], long long counts[4]);
 
+/* The CUDA stream (a cudaStream_t, returned as void*) on which this solver enqueues all
+ * of its work, so that callers can order their own work or record timing events on it.
+ * No counterpart in the reference (which runs on the legacy default stream). */
+int opo_get_stream(const OpoSolver *s, void **stream);
+
 int opo_synchronize(OpoSolver *s);
 int opo_round_trip_index(const OpoSolver *s);
 /* Number of kernels this solver has launched since creation (graph nodes included). */
