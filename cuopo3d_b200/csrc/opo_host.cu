@@ -198,11 +198,12 @@ struct DevBuf {
 };
 
 template <typename C> struct Tables {
+    using TT = typename opo::TabOf<C>::type;
     C *tw_t = nullptr, *tw_x = nullptr, *tw_y = nullptr;
-    C *disp[3] = {};       // t: dispersion
-    C *gddm[3] = {};       // t: GDD compensation and mirror (signal, idler)
-    C *dx[3] = {}, *dy[3] = {};     // x, y: crystal diffraction
-    C *fx[3] = {}, *fy[3] = {};     // x, y: free-space return
+    TT *disp[3] = {};       // t: dispersion
+    TT *gddm[3] = {};       // t: GDD compensation and mirror (signal, idler)
+    TT *dx[3] = {}, *dy[3] = {};     // x, y: crystal diffraction
+    TT *fx[3] = {}, *fy[3] = {};     // x, y: free-space return
 };
 
 }  // namespace
@@ -293,6 +294,11 @@ struct PassTimer {
 template <typename C> C to_c(const cd &v);
 template <> float2 to_c<float2>(const cd &v) { return make_float2((float)v.real(), (float)v.imag()); }
 template <> double2 to_c<double2>(const cd &v) { return make_double2(v.real(), v.imag()); }
+template <> float4 to_c<float4>(const cd &v)
+{
+    const float hx = (float)v.real(), hy = (float)v.imag();
+    return make_float4(hx, hy, (float)(v.real() - hx), (float)(v.imag() - hy));
+}
 
 template <typename C> int upload(OpoSolver *s, const std::vector<cd> &h, C **out)
 {
@@ -351,7 +357,7 @@ template <typename C> int setup_tables(OpoSolver *s)
             if (!phys) v *= std::exp(-0.5 * p.alpha[f] * p.dz);
             tab[pos] = v * (q2scale / nt);
         }
-        if ((rc = upload<C>(s, tab, &T->disp[f]))) return rc;
+        if ((rc = upload<typename Tables<C>::TT>(s, tab, &T->disp[f]))) return rc;
     }
     // t axis at the end of a round trip, signal and idler: GDD compensation
     // exp(i w^2 GDD / 2) (Solver3D.cuh:261-277, 676) times the mirror sqrt(R) e^{i phase}
@@ -365,7 +371,7 @@ template <typename C> int setup_tables(OpoSolver *s)
             const double wk = s->w[bin_of_position(s->plan_t, pos)];
             tab[pos] = std::polar(1.0, 0.5 * wk * wk * p.gdd) * mirror / (double)nt;
         }
-        if ((rc = upload<C>(s, tab, &T->gddm[f]))) return rc;
+        if ((rc = upload<typename Tables<C>::TT>(s, tab, &T->gddm[f]))) return rc;
     }
     // x, y: the diffraction propagator exp(sign L 2 pi^2 / k (fx^2 + fy^2)) of
     // Solver3D.cuh:282-323 factorised as (x factor)(y factor); fx = centred(i) / (dx nx).
@@ -387,8 +393,9 @@ template <typename C> int setup_tables(OpoSolver *s)
                       (q1scale / ny);
             fty[pos] = std::polar(1.0, p.free_len * cy * u * u) / (double)ny;
         }
-        if ((rc = upload<C>(s, tx, &T->dx[f])) || (rc = upload<C>(s, ty, &T->dy[f])) ||
-            (rc = upload<C>(s, ftx, &T->fx[f])) || (rc = upload<C>(s, fty, &T->fy[f])))
+        using TT = typename Tables<C>::TT;
+        if ((rc = upload<TT>(s, tx, &T->dx[f])) || (rc = upload<TT>(s, ty, &T->dy[f])) ||
+            (rc = upload<TT>(s, ftx, &T->fx[f])) || (rc = upload<TT>(s, fty, &T->fy[f])))
             return rc;
     }
     s->gdd_or_mirror = p.gdd != 0 || (p.resonant & 6u);
@@ -440,7 +447,8 @@ template <typename C> C *fld(OpoSolver *s, int k) { return static_cast<C *>(s->f
 // One t-pass.  n_rk4 half steps (z of each given), then, for the fields in tmask,
 // transform -> table -> inverse.
 template <typename C>
-int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, C *const *tab, unsigned tmask)
+int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh,
+              typename opo::TabOf<C>::type *const *tab, unsigned tmask)
 {
     const OpoParams &p = s->p;
     opo::TPassArgs<C> a{};
@@ -475,7 +483,8 @@ int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, C *con
     return OPO_OK;
 }
 
-template <typename C> int enqueue_axis(OpoSolver *s, bool xaxis, C *const *tab, unsigned mask)
+template <typename C>
+int enqueue_axis(OpoSolver *s, bool xaxis, typename opo::TabOf<C>::type *const *tab, unsigned mask)
 {
     opo::AxisArgs<C> a{};
     for (int f = 0; f < 3; f++) a.f[f] = fld<C>(s, f + 1);
@@ -537,7 +546,7 @@ template <typename C> int enqueue_single_pass(OpoSolver *s)
     int rc;
     if ((rc = enqueue_crystal<C>(s, false))) return rc;
     const double z = last_half_z<C>(s->p);
-    return enqueue_t<C>(s, false, 1, &z, nullptr, 0u);
+    return enqueue_t<C>(s, false, 1, &z, (typename opo::TabOf<C>::type *const *)nullptr, 0u);
 }
 
 // One round trip (Solver3D.cuh:979-997): fresh pump, crystal, final half step fused

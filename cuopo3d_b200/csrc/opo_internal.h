@@ -42,6 +42,12 @@ template <typename C> struct RealOf;
 template <> struct RealOf<float2> { using type = float; };
 template <> struct RealOf<double2> { using type = double; };
 
+// Phase-table entry: complex128 for FP64 fields; for FP32 fields a float4 (hi.x, hi.y,
+// lo.x, lo.y) with hi + lo equal to the FP64 value to ~1e-15, so that a table applied
+// every z-step carries no coherent FP32 rounding bias.
+template <typename C> struct TabOf { using type = C; };
+template <> struct TabOf<float2> { using type = float4; };
+
 template <typename C> struct TPassArgs {
     using T = typename RealOf<C>::type;
     C *f[3];            // pump, signal, idler (updated in place)
@@ -49,7 +55,7 @@ template <typename C> struct TPassArgs {
     TileGeom g;
     AxisPlan plan;
     const C *tw;        // stage twiddles of the t axis
-    const C *tab[3];    // phase table per field (digit-reversed order), used when in tmask
+    const typename TabOf<C>::type *tab[3];  // phase table per field (digit-reversed order)
     unsigned tmask;     // fields that get the t-axis transform
     int n_rk4;          // coupled-wave half steps before the transform (0, 1, 2)
     int use_phase;      // apply exp(-/+ i dk z) (corrected physics)
@@ -65,7 +71,7 @@ template <typename C> struct AxisArgs {
     TileGeom g;
     AxisPlan plan;
     const C *tw;
-    const C *tab[3];
+    const typename TabOf<C>::type *tab[3];
     unsigned tmask;
 };
 

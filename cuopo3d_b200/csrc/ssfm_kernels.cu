@@ -25,6 +25,13 @@ template <int S, typename C> __device__ __forceinline__ C twmul(C x, C w)
     return S < 0 ? cmul(x, w) : cmulc(x, w);
 }
 
+__device__ __forceinline__ double2 tab_mul(double2 x, double2 t) { return cmul(x, t); }
+__device__ __forceinline__ float2 tab_mul(float2 x, float4 t)
+{
+    const float2 a = cmul(x, make_float2(t.x, t.y)), b = cmul(x, make_float2(t.z, t.w));
+    return make_float2(a.x + b.x, a.y + b.y);
+}
+
 __device__ __forceinline__ long long tile_base(const TileGeom &g, int tile)
 {
     return (long long)(tile % g.tdiv) * g.tmulA + (long long)(tile / g.tdiv) * g.tmulB;
@@ -63,8 +70,8 @@ __device__ void smem_stage(C *sm, int LS, int nlines, int n, int L, const C *tw,
 
 // Last forward stage (q = 1), phase multiply, first inverse stage, in registers.
 template <typename C, int R, int SF>
-__device__ void fused_middle(C *sm, int LS, int nlines, int n, const C *const *tab, int nf,
-                             const int *fslot, const int *fid)
+__device__ void fused_middle(C *sm, int LS, int nlines, int n, const typename TabOf<C>::type *const *tab,
+                             int nf, const int *fslot, const int *fid)
 {
     const int nb = n / R;
     const int per_field = nb * nlines;
@@ -72,13 +79,13 @@ __device__ void fused_middle(C *sm, int LS, int nlines, int n, const C *const *t
         const int f = w / per_field, r = w - f * per_field;
         const int g = r / nlines, l = r - g * nlines;
         C *s = sm + (size_t)fslot[f] * n * LS + l;
-        const C *tb = tab[fid[f]] + g * R;
+        const typename TabOf<C>::type *tb = tab[fid[f]] + g * R;
         C x[R];
 #pragma unroll
         for (int m = 0; m < R; m++) x[m] = s[(g * R + m) * LS];
         dft<R, SF>(x);
 #pragma unroll
-        for (int k = 0; k < R; k++) x[k] = cmul(x[k], __ldg(tb + k));
+        for (int k = 0; k < R; k++) x[k] = tab_mul(x[k], __ldg(tb + k));
         dft<R, -SF>(x);
 #pragma unroll
         for (int k = 0; k < R; k++) s[(g * R + k) * LS] = x[k];
@@ -100,8 +107,9 @@ __device__ void smem_stage_dispatch(int R, C *sm, int LS, int nlines, int n, int
 }
 
 template <typename C, int SF>
-__device__ void fused_dispatch(int R, C *sm, int LS, int nlines, int n, const C *const *tab,
-                               int nf, const int *fslot, const int *fid)
+__device__ void fused_dispatch(int R, C *sm, int LS, int nlines, int n,
+                               const typename TabOf<C>::type *const *tab, int nf, const int *fslot,
+                               const int *fid)
 {
     switch (R) {
     case 2: fused_middle<C, 2, SF>(sm, LS, nlines, n, tab, nf, fslot, fid); break;
@@ -117,7 +125,8 @@ __device__ void fused_dispatch(int R, C *sm, int LS, int nlines, int n, const C 
 // with the global load / store by the caller).
 template <typename C, int SF>
 __device__ void middle_stages(C *sm, const TileGeom &g, const AxisPlan &p, const C *tw,
-                              const C *const *tab, int nf, const int *fslot, const int *fid)
+                              const typename TabOf<C>::type *const *tab, int nf, const int *fslot,
+                              const int *fid)
 {
     for (int s = 1; s < p.ns - 1; s++) {
         smem_stage_dispatch<C, SF, false>(p.radix[s], sm, g.LS, g.nlines, p.n, p.len[s],
