@@ -86,6 +86,7 @@ def lib():
         L.opo_field_sums.argtypes = [vp, dp]
         L.opo_synchronize.argtypes = [vp]
         L.opo_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.opo_field_sums_noalloc.argtypes = [vp, vp, vp, ctypes.c_size_t, _i, vp, dp]
         L.opo_set_pass_timing.argtypes = [vp, _i]
         L.opo_pass_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong)]
         L.opo_round_trip_index.argtypes = [vp]

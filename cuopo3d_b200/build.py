@@ -9,7 +9,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libcuopo3d.so")
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("ssfm_kernels.cu", "opo_host.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("ssfm_kernels.cu", "opo_host.cu", "noalloc_sums.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fft_radix.cuh", "opo_internal.h")] + [
     os.path.join(ROOT, "include", "cuopo3d.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -183,6 +183,21 @@ int opo_pass_times(OpoSolver *s, double ms[4], long long counts[4]);
  * No counterpart in the reference (which runs on the legacy default stream). */
 int opo_get_stream(const OpoSolver *s, void **stream);
 
+/* Allocation-free FP64 tallies: the same three sums of |A|^2 as opo_field_sums, over
+ * caller-owned device fields f0, f1, f2 of n complex values each (precision OPO_FP32 or
+ * OPO_FP64), enqueued on `stream` (a cudaStream_t, or NULL for the legacy stream); the
+ * call waits for the stream and writes the sums to host memory.  For callers that
+ * cannot call cudaMalloc -- hosts whose own allocator has reserved the device memory,
+ * or loops that cannot afford an allocation's implicit device synchronisation -- it
+ * allocates nothing: its scratch is a fixed 98,328-byte device array inside the library,
+ * held on every device that loads it until exit.  Limit: n <= 268,435,456 values per
+ * field, larger n returns OPO_ERR_CAPACITY.  All calls share that array, so calls whose
+ * GPU work overlaps race and must be ordered by the caller.  The first call on a device
+ * looks up the array's device address; make that first call before any stream capture.
+ * This entry point has no counterpart in the reference. */
+int opo_field_sums_noalloc(const void *f0, const void *f1, const void *f2, size_t n, int precision,
+                           void *stream, double sums[3]);
+
 int opo_synchronize(OpoSolver *s);
 int opo_round_trip_index(const OpoSolver *s);
 /* Number of kernels this solver has launched since creation (graph nodes included). */
