@@ -86,6 +86,8 @@ def lib():
         L.opo_field_sums.argtypes = [vp, dp]
         L.opo_synchronize.argtypes = [vp]
         L.opo_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.opo_autotune.argtypes = [vp]
+        L.opo_get_tuning.argtypes = [vp, ctypes.POINTER(_i)]
         L.opo_field_sums_noalloc.argtypes = [vp, vp, vp, ctypes.c_size_t, _i, vp, dp]
         L.opo_set_pass_timing.argtypes = [vp, _i]
         L.opo_pass_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong)]
@@ -213,6 +215,18 @@ class Simulation:
         st = ctypes.c_void_p()
         self._check(lib().opo_get_stream(self._h, ctypes.byref(st)))
         return st.value or 0
+
+    def autotune(self):
+        """Pick the fastest kernel variant and tile per pass (zeroes Ap, As, Ai)."""
+        self._check(lib().opo_autotune(self._h))
+        return self.tuning
+
+    @property
+    def tuning(self):
+        out = (_i * 9)()
+        self._check(lib().opo_get_tuning(self._h, out))
+        return {k: dict(threads=out[3 * i], tile=out[3 * i + 1], r1=out[3 * i + 2])
+                for i, k in enumerate(("t", "x", "y"))}
 
     def set_pass_timing(self, enable):
         self._check(lib().opo_set_pass_timing(self._h, 1 if enable else 0))

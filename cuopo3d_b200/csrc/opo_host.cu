@@ -9,6 +9,7 @@
 #include <complex>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -124,37 +125,55 @@ int zloop_steps(double Lcr, double dz, bool f32)
 // ---------------------------------------------------------------------------------
 // FFT stage plans and tables.
 
-bool split_pow2(int e, std::vector<int> &out)
+opo::FastDiv make_fastdiv(unsigned d)
 {
-    // radices for 2^e, largest first, balanced (16, 8, 4, 2)
-    static const int table[][3] = {{0, 0, 0}, {2, 0, 0}, {4, 0, 0}, {8, 0, 0}, {16, 0, 0}, {8, 4, 0},
-                                   {8, 8, 0}, {16, 8, 0}, {16, 16, 0}, {8, 8, 8}, {16, 8, 8}, {16, 16, 8},
-                                   {16, 16, 16}};
+    opo::FastDiv f{d ? d : 1u, 0u, 0u};
+    unsigned l = 0;
+    while ((1ull << l) < f.d) l++;
+    if ((1ull << l) == f.d) {
+        f.s = l;
+        return f;
+    }
+    f.m = (unsigned)(((1ull << (31 + l)) + f.d - 1) / f.d);
+    f.s = l - 1;
+    return f;
+}
+
+// Radices for 2^e, each <= rmax, largest first and balanced.
+bool split_pow2(int e, int rmax, std::vector<int> &out)
+{
+    static const int t16[][3] = {{0, 0, 0}, {2, 0, 0}, {4, 0, 0}, {8, 0, 0}, {16, 0, 0}, {8, 4, 0},
+                                 {8, 8, 0}, {16, 8, 0}, {16, 16, 0}, {8, 8, 8}, {16, 8, 8}, {16, 16, 8},
+                                 {16, 16, 16}};
+    static const int t8[][4] = {{0, 0, 0, 0}, {2, 0, 0, 0}, {4, 0, 0, 0}, {8, 0, 0, 0}, {4, 4, 0, 0},
+                                {8, 4, 0, 0}, {8, 8, 0, 0}, {8, 4, 4, 0}, {8, 8, 4, 0}, {8, 8, 8, 0},
+                                {8, 8, 4, 4}, {8, 8, 8, 4}, {8, 8, 8, 8}};
     if (e < 0 || e > 12) return false;
-    for (int k = 0; k < 3; k++)
-        if (table[e][k]) out.push_back(table[e][k]);
+    if (rmax >= 16) {
+        for (int k = 0; k < 3; k++)
+            if (t16[e][k]) out.push_back(t16[e][k]);
+    } else {
+        for (int k = 0; k < 4; k++)
+            if (t8[e][k]) out.push_back(t8[e][k]);
+    }
     return true;
 }
 
-// n = 2^a 3^b, first-stage radix r1 (a power of two dividing n).
-bool build_plan(int n, int r1_max, opo::AxisPlan &p, std::vector<cd> &tw)
+// Plan for n = 2^a 3^b with first-stage radix r1 (a power of two >= 4 dividing n, with
+// at least one more stage after it) and every other radix <= rmax.
+bool build_plan(int n, int r1, int rmax, opo::AxisPlan &p, std::vector<cd> &tw)
 {
-    if (n < 4) return false;
-    int a = 0, b = 0, m = n;
+    if (n < 8 || r1 < 4 || (r1 & (r1 - 1)) || n % r1 || n / r1 < 2) return false;
+    int a = 0, b = 0, m = n / r1;
     while (m % 2 == 0) { m /= 2; a++; }
     while (m % 3 == 0) { m /= 3; b++; }
     if (m != 1) return false;
-    int r1 = 1, e1 = 0;
-    while (r1 * 2 <= r1_max && e1 < a) { r1 *= 2; e1++; }
-    // keep at least one more stage
-    while (e1 > 0 && n / r1 < 2) { r1 /= 2; e1--; }
-    if (r1 < 4 && a >= 2) { r1 = 4; e1 = 2; }
-    if (r1 < 4) return false;  // first stage needs a power-of-two radix >= 4
     std::vector<int> rad;
     rad.push_back(r1);
     for (int k = 0; k < b; k++) rad.push_back(3);
-    if (!split_pow2(a - e1, rad)) return false;
+    if (!split_pow2(a, rmax, rad)) return false;
     if (rad.size() < 2 || (int)rad.size() > opo::kMaxStages) return false;
+    p = opo::AxisPlan{};
     p.n = n;
     p.ns = (int)rad.size();
     tw.clear();
@@ -164,6 +183,7 @@ bool build_plan(int n, int r1_max, opo::AxisPlan &p, std::vector<cd> &tw)
         p.radix[s] = R;
         p.len[s] = L;
         p.twoff[s] = (int)tw.size();
+        p.q[s] = make_fastdiv((unsigned)q);
         for (int k = 1; k < R; k++)
             for (int j = 0; j < q; j++) tw.push_back(std::polar(1.0, -2 * kPi * (double)j * k / L));
         L = q;
@@ -190,20 +210,20 @@ int bin_of_position(const opo::AxisPlan &p, int pos)
 // (EFields3D.cuh:141-171): (i + n/2) mod n - n/2.
 double centred(int i, int n) { return (double)((i + n / 2) % n) - 0.5 * n; }
 
-// ---------------------------------------------------------------------------------
+enum PassKind { kT = 0, kX = 1, kY = 2 };
 
-struct DevBuf {
-    void *p = nullptr;
-    size_t bytes = 0;
-};
-
-template <typename C> struct Tables {
-    using TT = typename opo::TabOf<C>::type;
-    C *tw_t = nullptr, *tw_x = nullptr, *tw_y = nullptr;
-    TT *disp[3] = {};       // t: dispersion
-    TT *gddm[3] = {};       // t: GDD compensation and mirror (signal, idler)
-    TT *dx[3] = {}, *dy[3] = {};     // x, y: crystal diffraction
-    TT *fx[3] = {}, *fy[3] = {};     // x, y: free-space return
+// Configuration of one pass kind: kernel variant, tile size, FFT plan, tile geometry
+// and the device tables built for that plan ([0] crystal step, [1] round-trip
+// boundary: GDD + mirrors for t, free space for x and y).
+struct PassCfg {
+    opo::PassVariant v{256, 16};
+    size_t te = 0;
+    opo::AxisPlan plan{};
+    opo::TileGeom geo{};
+    size_t smem = 0;
+    void *tw = nullptr;
+    void *tab[2][3] = {};
+    std::vector<void *> allocs;
 };
 
 }  // namespace
@@ -216,12 +236,7 @@ struct OpoSolver {
     size_t V = 0;
     size_t esz = 0;  // bytes per complex element
     void *field[4] = {};  // Api, Ap, As, Ai
-    std::vector<void *> allocs;
-    opo::AxisPlan plan_t{}, plan_x{}, plan_y{};
-    int r1_t = 0, r1_x = 0, r1_y = 0;
-    opo::TileGeom geo_t{}, geo_x{}, geo_y{};
-    size_t smem_t = 0, smem_x = 0, smem_y = 0;
-    void *tables = nullptr;   // Tables<C>*
+    PassCfg pass[3];
     std::vector<double> w;
     double *partials = nullptr, *sums_dev = nullptr;
     int sum_blocks = 0;
@@ -300,15 +315,16 @@ template <> float4 to_c<float4>(const cd &v)
     return make_float4(hx, hy, (float)(v.real() - hx), (float)(v.imag() - hy));
 }
 
-template <typename C> int upload(OpoSolver *s, const std::vector<cd> &h, C **out)
+template <typename C> int upload(OpoSolver *s, PassCfg &pc, const std::vector<cd> &h, void **out)
 {
     std::vector<C> tmp(h.size());
     for (size_t k = 0; k < h.size(); k++) tmp[k] = to_c<C>(h[k]);
     void *d = nullptr;
-    OPO_CU(s, cudaMalloc(&d, sizeof(C) * tmp.size()), "cudaMalloc(table)");
-    s->allocs.push_back(d);
-    OPO_CU(s, cudaMemcpy(d, tmp.data(), sizeof(C) * tmp.size(), cudaMemcpyHostToDevice), "cudaMemcpy(table)");
-    *out = static_cast<C *>(d);
+    OPO_CU(s, cudaMalloc(&d, sizeof(C) * (tmp.size() ? tmp.size() : 1)), "cudaMalloc(table)");
+    pc.allocs.push_back(d);
+    if (!tmp.empty())
+        OPO_CU(s, cudaMemcpy(d, tmp.data(), sizeof(C) * tmp.size(), cudaMemcpyHostToDevice), "cudaMemcpy(table)");
+    *out = d;
     return OPO_OK;
 }
 
@@ -320,146 +336,165 @@ int largest_divisor_leq(int n, int cap)
     return 1;
 }
 
-// Tile elements per field: 96 KB of shared memory for the three fields in either
-// precision, two CTAs per SM.
-size_t tile_elems(int precision) { return precision == OPO_FP64 ? 2048 : 4096; }
+void free_pass(PassCfg &pc)
+{
+    for (auto *a : pc.allocs) cudaFree(a);
+    pc.allocs.clear();
+    pc.tw = nullptr;
+    for (auto &row : pc.tab)
+        for (auto &t : row) t = nullptr;
+}
 
-template <typename C> int setup_tables(OpoSolver *s)
+void drop_graphs(OpoSolver *s)
+{
+    for (auto &g : s->graph_rt)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+// Default variant and tile size of a pass kind: 96 KB of shared memory for the three
+// fields (4096 complex64 or 2048 complex128 per field), 256 threads.
+void default_variant(bool fp64, int kind, opo::PassVariant &v, size_t &te)
+{
+    v.threads = 256;
+    v.r1 = (fp64 && kind == kT) ? 8 : 16;
+    te = fp64 ? 2048 : 4096;
+}
+
+// Build the plan, geometry and tables of one pass kind for variant v and tile size te.
+template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVariant v, size_t te)
 {
     const OpoParams &p = s->p;
-    auto *T = new (std::nothrow) Tables<C>();
-    if (!T) return fail(s, OPO_ERR_NOMEM, "host allocation");
-    s->tables = T;
-    std::vector<cd> twt, twx, twy;
-    const int r1max_t = sizeof(C) == 8 ? 16 : 8;
-    if (!build_plan(p.nt, r1max_t, s->plan_t, twt) || !build_plan(p.nx, 16, s->plan_x, twx) ||
-        !build_plan(p.ny, 16, s->plan_y, twy))
-        return fail(s, OPO_ERR_INVALID, "grid sizes must be 2^a 3^b and >= 4");
-    s->r1_t = s->plan_t.radix[0];
-    s->r1_x = s->plan_x.radix[0];
-    s->r1_y = s->plan_y.radix[0];
-    int rc;
-    if ((rc = upload<C>(s, twt, &T->tw_t)) || (rc = upload<C>(s, twx, &T->tw_x)) ||
-        (rc = upload<C>(s, twy, &T->tw_y)))
-        return rc;
-
-    const bool phys = (p.flags & OPO_PHYSICS) != 0;
+    const bool fp64 = sizeof(C) == 16;
+    using TT = typename opo::TabOf<C>::type;
+    PassCfg pc;
+    pc.v = v;
+    pc.te = te;
     const int nx = p.nx, ny = p.ny, nt = p.nt;
-    // t axis: dispersion exp(i dz w (vinv + w b2/2)) exp(-alpha dz/2) / nt
-    // (Solver3D.cuh:153-169; the 1/nt of the inverse transform folded in), placed at the
-    // digit-reversed positions of the t plan.
-    const double q2scale = (p.flags & OPO_ASIS_Q2) ? 1.0 / ((double)nx * ny) : 1.0;
-    for (int f = 0; f < 3; f++) {
-        std::vector<cd> tab(nt);
-        for (int pos = 0; pos < nt; pos++) {
-            const double wk = s->w[bin_of_position(s->plan_t, pos)];
-            cd v = std::polar(1.0, p.dz * wk * (p.vinv[f] + 0.5 * wk * p.beta2[f]));
-            if (!phys) v *= std::exp(-0.5 * p.alpha[f] * p.dz);
-            tab[pos] = v * (q2scale / nt);
-        }
-        if ((rc = upload<typename Tables<C>::TT>(s, tab, &T->disp[f]))) return rc;
-    }
-    // t axis at the end of a round trip, signal and idler: GDD compensation
-    // exp(i w^2 GDD / 2) (Solver3D.cuh:261-277, 676) times the mirror sqrt(R) e^{i phase}
-    // (Cavity3D.cuh:12-28) for resonant fields, / nt.
-    for (int f = 1; f < 3; f++) {
-        const bool res = (p.resonant >> f) & 1u;
-        const double R = f == 1 ? p.Rs : p.Ri;
-        const cd mirror = res ? std::sqrt(R) * std::polar(1.0, p.detuning) : cd(1, 0);
-        std::vector<cd> tab(nt);
-        for (int pos = 0; pos < nt; pos++) {
-            const double wk = s->w[bin_of_position(s->plan_t, pos)];
-            tab[pos] = std::polar(1.0, 0.5 * wk * wk * p.gdd) * mirror / (double)nt;
-        }
-        if ((rc = upload<typename Tables<C>::TT>(s, tab, &T->gddm[f]))) return rc;
-    }
-    // x, y: the diffraction propagator exp(sign L 2 pi^2 / k (fx^2 + fy^2)) of
-    // Solver3D.cuh:282-323 factorised as (x factor)(y factor); fx = centred(i) / (dx nx).
-    // The crystal y factor carries exp(-alpha dz / 2) and the 1/(nx ny) normalisation is
-    // split as 1/nx, 1/ny (shipped 1/(nx ny nt) with OPO_ASIS_Q1).
-    const double q1scale = (p.flags & OPO_ASIS_Q1) ? 1.0 / nt : 1.0;
-    for (int f = 0; f < 3; f++) {
-        const double cx = 2 * kPi * kPi / p.kdiff[f] / (p.dx * nx) / (p.dx * nx);
-        const double cy = 2 * kPi * kPi / p.kdiff[f] / (p.dy * ny) / (p.dy * ny);
-        std::vector<cd> tx(nx), ty(ny), ftx(nx), fty(ny);
-        for (int pos = 0; pos < nx; pos++) {
-            const double u = centred(bin_of_position(s->plan_x, pos), nx);
-            tx[pos] = std::polar(1.0, -p.dz * cx * u * u) / (double)nx;
-            ftx[pos] = std::polar(1.0, p.free_len * cx * u * u) / (double)nx;
-        }
-        for (int pos = 0; pos < ny; pos++) {
-            const double u = centred(bin_of_position(s->plan_y, pos), ny);
-            ty[pos] = std::polar(1.0, -p.dz * cy * u * u) * std::exp(-0.5 * p.alpha[f] * p.dz) *
-                      (q1scale / ny);
-            fty[pos] = std::polar(1.0, p.free_len * cy * u * u) / (double)ny;
-        }
-        using TT = typename Tables<C>::TT;
-        if ((rc = upload<TT>(s, tx, &T->dx[f])) || (rc = upload<TT>(s, ty, &T->dy[f])) ||
-            (rc = upload<TT>(s, ftx, &T->fx[f])) || (rc = upload<TT>(s, fty, &T->fy[f])))
-            return rc;
-    }
-    s->gdd_or_mirror = p.gdd != 0 || (p.resonant & 6u);
-
-    // Tile geometry.
-    const size_t TE = tile_elems(p.precision);
-    const long long nxy = (long long)nx * ny;
-    {
-        const int P = largest_divisor_leq(nx, (int)(TE / nt));
-        if (P < 1 || (size_t)nt > TE) return fail(s, OPO_ERR_INVALID, "nt too large for one tile");
-        opo::TileGeom &g = s->geo_t;
-        g.nlines = P; g.LS = P; g.ntiles = (nx / P) * ny; g.tdiv = nx / P;
-        g.tmulA = P; g.tmulB = nx; g.gs_j = nxy; g.gs_l = 1;
-        s->smem_t = 3 * (size_t)nt * g.LS * sizeof(C);
-    }
-    {
-        const int Py = largest_divisor_leq(nx, (int)(TE / ny));
-        if (Py < 1 || (size_t)ny > TE) return fail(s, OPO_ERR_INVALID, "ny too large for one tile");
-        opo::TileGeom &g = s->geo_y;
-        g.nlines = Py; g.LS = Py; g.ntiles = (nx / Py) * nt; g.tdiv = nx / Py;
-        g.tmulA = Py; g.tmulB = nxy; g.gs_j = nx; g.gs_l = 1;
-        s->smem_y = 3 * (size_t)ny * g.LS * sizeof(C);
-    }
-    {
-        const int rows = largest_divisor_leq(ny * nt, (int)(TE / nx));
-        if (rows < 1 || (size_t)nx > TE) return fail(s, OPO_ERR_INVALID, "nx too large for one tile");
-        opo::TileGeom &g = s->geo_x;
+    const int n = kind == kT ? nt : (kind == kX ? nx : ny);
+    if ((size_t)n > te) return fail(s, OPO_ERR_INVALID, "axis longer than the tile");
+    std::vector<cd> tw;
+    int r1 = v.r1;
+    if (fp64 && kind == kT && r1 > 8) r1 = 8;  // 3 fields x r1 complex128 live in registers
+    while (r1 >= 4 && !build_plan(n, r1, opo::max_radix(fp64, v.threads), pc.plan, tw)) r1 /= 2;
+    if (r1 < 4) return fail(s, OPO_ERR_INVALID, "grid sizes must be 2^a 3^b and >= 8");
+    pc.v.r1 = r1;
+    const unsigned nxy = (unsigned)nx * ny;
+    opo::TileGeom &g = pc.geo;
+    if (kind == kT) {
+        const int P = largest_divisor_leq(nx, (int)(te / nt));
+        g.nlines = P; g.LS = P; g.ntiles = (nx / P) * ny;
+        g.tdiv = make_fastdiv(nx / P); g.tmulA = P; g.tmulB = nx; g.gs_j = nxy; g.gs_l = 1;
+    } else if (kind == kY) {
+        const int Py = largest_divisor_leq(nx, (int)(te / ny));
+        g.nlines = Py; g.LS = Py; g.ntiles = (nx / Py) * nt;
+        g.tdiv = make_fastdiv(nx / Py); g.tmulA = Py; g.tmulB = nxy; g.gs_j = nx; g.gs_l = 1;
+    } else {
+        const int rows = largest_divisor_leq(ny * nt, (int)(te / nx));
         g.nlines = rows;
         // Pad the line stride so that the consecutive-butterfly mapping of the first
         // and last stages is bank-conflict free: a conflict-free unit holds 128 B
         // (16 complex64 or 8 complex128); with q' = min(nx/R1, unit) consecutive
-        // butterflies per line, LS = 0 mod (unit/q') makes b LS + l distinct.
-        const int unit = sizeof(C) == 8 ? 16 : 8;
-        int qq = nx / s->r1_x;
+        // butterflies per line, LS = unit/q' mod unit makes b LS + l distinct.
+        const int unit = fp64 ? 8 : 16;
+        int qq = nx / r1;
         if (qq > unit) qq = unit;
         const int step = unit / qq;
         int LS = rows;
         while ((LS % unit) != (step % unit)) LS++;
         g.LS = LS;
-        g.ntiles = ny * nt / rows; g.tdiv = 1;
-        g.tmulA = 0; g.tmulB = (long long)rows * nx; g.gs_j = 1; g.gs_l = nx;
-        s->smem_x = 3 * (size_t)nx * g.LS * sizeof(C);
+        g.ntiles = ny * nt / rows;
+        g.tdiv = make_fastdiv(1); g.tmulA = 0; g.tmulB = (unsigned)rows * nx; g.gs_j = 1; g.gs_l = nx;
     }
+    g.nl = make_fastdiv((unsigned)g.nlines);
+    pc.smem = 3 * (size_t)n * g.LS * sizeof(C);
+    if (pc.smem > 227 * 1024) return fail(s, OPO_ERR_INVALID, "tile does not fit in shared memory");
+
+    int rc;
+    if ((rc = upload<C>(s, pc, tw, &pc.tw))) { free_pass(pc); return rc; }
+    const bool phys = (p.flags & OPO_PHYSICS) != 0;
+    const opo::AxisPlan &pl = pc.plan;
+    if (kind == kT) {
+        // dispersion exp(i dz w (vinv + w b2/2)) exp(-alpha dz/2) / nt (Solver3D.cuh:153-169,
+        // with the 1/nt of the inverse transform folded in)
+        const double q2scale = (p.flags & OPO_ASIS_Q2) ? 1.0 / ((double)nx * ny) : 1.0;
+        for (int f = 0; f < 3; f++) {
+            std::vector<cd> tab(nt);
+            for (int pos = 0; pos < nt; pos++) {
+                const double wk = s->w[bin_of_position(pl, pos)];
+                cd v = std::polar(1.0, p.dz * wk * (p.vinv[f] + 0.5 * wk * p.beta2[f]));
+                if (!phys) v *= std::exp(-0.5 * p.alpha[f] * p.dz);
+                tab[pos] = v * (q2scale / nt);
+            }
+            if ((rc = upload<TT>(s, pc, tab, &pc.tab[0][f]))) { free_pass(pc); return rc; }
+        }
+        // GDD compensation exp(i w^2 GDD / 2) (Solver3D.cuh:261-277, 676) times the mirror
+        // sqrt(R) e^{i phase} (Cavity3D.cuh:12-28) for resonant signal / idler, / nt
+        for (int f = 1; f < 3; f++) {
+            const bool res = (p.resonant >> f) & 1u;
+            const double R = f == 1 ? p.Rs : p.Ri;
+            const cd mirror = res ? std::sqrt(R) * std::polar(1.0, p.detuning) : cd(1, 0);
+            std::vector<cd> tab(nt);
+            for (int pos = 0; pos < nt; pos++) {
+                const double wk = s->w[bin_of_position(pl, pos)];
+                tab[pos] = std::polar(1.0, 0.5 * wk * wk * p.gdd) * mirror / (double)nt;
+            }
+            if ((rc = upload<TT>(s, pc, tab, &pc.tab[1][f]))) { free_pass(pc); return rc; }
+        }
+    } else {
+        // the propagator exp(sign L 2 pi^2 / k (fx^2 + fy^2)) of Solver3D.cuh:282-323
+        // factorised as (x factor)(y factor); fx = centred(i) / (dx nx).  The crystal y
+        // factor carries exp(-alpha dz / 2); the 1/(nx ny) normalisation is split as 1/nx,
+        // 1/ny (shipped 1/(nx ny nt) with OPO_ASIS_Q1).
+        const bool xa = kind == kX;
+        const double q1scale = (!xa && (p.flags & OPO_ASIS_Q1)) ? 1.0 / nt : 1.0;
+        for (int f = 0; f < 3; f++) {
+            const double d = xa ? p.dx : p.dy;
+            const double c = 2 * kPi * kPi / p.kdiff[f] / (d * n) / (d * n);
+            std::vector<cd> crys(n), free(n);
+            for (int pos = 0; pos < n; pos++) {
+                const double u = centred(bin_of_position(pl, pos), n);
+                cd v = std::polar(1.0, -p.dz * c * u * u) / (double)n;
+                if (!xa) v *= std::exp(-0.5 * p.alpha[f] * p.dz) * q1scale;
+                crys[pos] = v;
+                free[pos] = std::polar(1.0, p.free_len * c * u * u) / (double)n;
+            }
+            if ((rc = upload<TT>(s, pc, crys, &pc.tab[0][f])) || (rc = upload<TT>(s, pc, free, &pc.tab[1][f]))) {
+                free_pass(pc);
+                return rc;
+            }
+        }
+    }
+    drop_graphs(s);
+    free_pass(s->pass[kind]);
+    s->pass[kind] = pc;
     return OPO_OK;
 }
 
 template <typename C> C *fld(OpoSolver *s, int k) { return static_cast<C *>(s->field[k]); }
 
+template <typename C> typename opo::TabOf<C>::type *const *tabs(OpoSolver *s, int kind, int which)
+{
+    return reinterpret_cast<typename opo::TabOf<C>::type *const *>(s->pass[kind].tab[which]);
+}
+
 // One t-pass.  n_rk4 half steps (z of each given), then, for the fields in tmask,
 // transform -> table -> inverse.
 template <typename C>
-int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh,
-              typename opo::TabOf<C>::type *const *tab, unsigned tmask)
+int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, int which_tab, unsigned tmask)
 {
     const OpoParams &p = s->p;
+    const PassCfg &pc = s->pass[kT];
     opo::TPassArgs<C> a{};
     using T = typename opo::TPassArgs<C>::T;
     for (int f = 0; f < 3; f++) a.f[f] = fld<C>(s, f + 1);
     a.psrc = reset_pump ? fld<C>(s, 0) : fld<C>(s, 1);
-    a.g = s->geo_t;
-    a.plan = s->plan_t;
-    auto *Tb = static_cast<Tables<C> *>(s->tables);
-    a.tw = Tb->tw_t;
-    for (int f = 0; f < 3; f++) a.tab[f] = tab ? tab[f] : nullptr;
+    a.g = pc.geo;
+    a.plan = pc.plan;
+    a.tw = static_cast<const C *>(pc.tw);
+    for (int f = 0; f < 3; f++) a.tab[f] = tabs<C>(s, kT, which_tab)[f];
     a.tmask = tmask;
     a.n_rk4 = n_rk4;
     const bool phys = (p.flags & OPO_PHYSICS) != 0;
@@ -475,29 +510,25 @@ int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh,
         for (int j = 0; j < 3; j++) a.ph[k][j] = to_c<C>(std::polar(1.0, p.dk * zs[j]));
     }
     a.skip_rows = (p.flags & OPO_ASIS_Q2) ? 1 : 0;
-    a.nx = p.nx;
-    int grid = a.g.ntiles;
+    a.nx = (unsigned)p.nx;
     PassTimer timer(s, 0);
-    OPO_CU(s, opo::launch_tpass<C>(a, s->r1_t, grid, s->smem_t, s->stream), "t-pass launch");
+    OPO_CU(s, opo::launch_tpass<C>(a, pc.v, a.g.ntiles, pc.smem, s->stream), "t-pass launch");
     s->launches++;
     return OPO_OK;
 }
 
-template <typename C>
-int enqueue_axis(OpoSolver *s, bool xaxis, typename opo::TabOf<C>::type *const *tab, unsigned mask)
+template <typename C> int enqueue_axis(OpoSolver *s, int kind, int which_tab, unsigned mask)
 {
+    const PassCfg &pc = s->pass[kind];
     opo::AxisArgs<C> a{};
     for (int f = 0; f < 3; f++) a.f[f] = fld<C>(s, f + 1);
-    auto *Tb = static_cast<Tables<C> *>(s->tables);
-    a.g = xaxis ? s->geo_x : s->geo_y;
-    a.plan = xaxis ? s->plan_x : s->plan_y;
-    a.tw = xaxis ? Tb->tw_x : Tb->tw_y;
-    for (int f = 0; f < 3; f++) a.tab[f] = tab[f];
+    a.g = pc.geo;
+    a.plan = pc.plan;
+    a.tw = static_cast<const C *>(pc.tw);
+    for (int f = 0; f < 3; f++) a.tab[f] = tabs<C>(s, kind, which_tab)[f];
     a.tmask = mask;
-    const int r1 = xaxis ? s->r1_x : s->r1_y;
-    const size_t smem = xaxis ? s->smem_x : s->smem_y;
-    PassTimer timer(s, xaxis ? 1 : 2);
-    OPO_CU(s, opo::launch_axis<C>(a, r1, xaxis, a.g.ntiles, smem, s->stream), "axis-pass launch");
+    PassTimer timer(s, kind);
+    OPO_CU(s, opo::launch_axis<C>(a, pc.v, kind == kX, a.g.ntiles, pc.smem, s->stream), "axis-pass launch");
     s->launches++;
     return OPO_OK;
 }
@@ -507,11 +538,10 @@ double step_z(const OpoParams &p, int k) { return k * p.dz; }
 
 // The crystal: for k in [0, n): RK4(h) D F RK4(h) (Solver3D.cuh:946-960), with
 // D the t-axis operator and F the (x,y) one.  Passes: T(N D), X, Y, then for each
-// later step T(N N D), X, Y; the final N is left to the caller (end_pass).
+// later step T(N N D), X, Y; the final N is left to the caller.
 template <typename C> int enqueue_crystal(OpoSolver *s, bool reset_pump)
 {
     const OpoParams &p = s->p;
-    auto *Tb = static_cast<Tables<C> *>(s->tables);
     const bool disp = (p.flags & OPO_DISPERSION) != 0, diff = (p.flags & OPO_DIFFRACTION) != 0;
     const bool phys = (p.flags & OPO_PHYSICS) != 0;
     int rc;
@@ -526,16 +556,16 @@ template <typename C> int enqueue_crystal(OpoSolver *s, bool reset_pump)
             zh[1] = step_z(p, k);
             nrk = 2;
         }
-        if ((rc = enqueue_t<C>(s, reset_pump && k == 0, nrk, zh, Tb->disp, disp ? 7u : 0u))) return rc;
+        if ((rc = enqueue_t<C>(s, reset_pump && k == 0, nrk, zh, 0, disp ? 7u : 0u))) return rc;
         if (diff) {
-            if ((rc = enqueue_axis<C>(s, true, Tb->dx, 7u))) return rc;
-            if ((rc = enqueue_axis<C>(s, false, Tb->dy, 7u))) return rc;
+            if ((rc = enqueue_axis<C>(s, kX, 0, 7u))) return rc;
+            if ((rc = enqueue_axis<C>(s, kY, 0, 7u))) return rc;
         }
     }
     return OPO_OK;
 }
 
-template <typename C> double last_half_z(const OpoParams &p)
+double last_half_z(const OpoParams &p)
 {
     const int k = p.n_steps - 1;
     return (p.flags & OPO_PHYSICS) ? step_z(p, k) + 0.5 * p.dz : step_z(p, k);
@@ -545,8 +575,8 @@ template <typename C> int enqueue_single_pass(OpoSolver *s)
 {
     int rc;
     if ((rc = enqueue_crystal<C>(s, false))) return rc;
-    const double z = last_half_z<C>(s->p);
-    return enqueue_t<C>(s, false, 1, &z, (typename opo::TabOf<C>::type *const *)nullptr, 0u);
+    const double z = last_half_z(s->p);
+    return enqueue_t<C>(s, false, 1, &z, 0, 0u);
 }
 
 // One round trip (Solver3D.cuh:979-997): fresh pump, crystal, final half step fused
@@ -556,18 +586,13 @@ template <typename C> int enqueue_single_pass(OpoSolver *s)
 template <typename C> int enqueue_round_trip(OpoSolver *s, bool last)
 {
     const OpoParams &p = s->p;
-    auto *Tb = static_cast<Tables<C> *>(s->tables);
     int rc;
     if ((rc = enqueue_crystal<C>(s, true))) return rc;
-    const double z = last_half_z<C>(p);
-    const bool disp = (p.flags & OPO_DISPERSION) != 0;
-    unsigned m = 0;
-    if (s->gdd_or_mirror) m = 6u;
-    if ((rc = enqueue_t<C>(s, false, 1, &z, Tb->gddm, m))) return rc;
-    (void)disp;
+    const double z = last_half_z(p);
+    if ((rc = enqueue_t<C>(s, false, 1, &z, 1, s->gdd_or_mirror ? 6u : 0u))) return rc;
     if (!last && (p.flags & OPO_DIFFRACTION)) {
-        if ((rc = enqueue_axis<C>(s, true, Tb->fx, 6u))) return rc;
-        if ((rc = enqueue_axis<C>(s, false, Tb->fy, 6u))) return rc;
+        if ((rc = enqueue_axis<C>(s, kX, 1, 6u))) return rc;
+        if ((rc = enqueue_axis<C>(s, kY, 1, 6u))) return rc;
     }
     return OPO_OK;
 }
@@ -627,6 +652,100 @@ template <typename C> int field_sums(OpoSolver *s, double out[3])
     OPO_CU(s, cudaStreamSynchronize(s->stream), "sums sync");
     for (int k = 0; k < 3; k++)
         if (!std::isfinite(out[k])) return fail(s, OPO_ERR_NONFINITE, "a field is not finite");
+    return OPO_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Autotuner: per pass kind, time every compiled variant x tile size that fits and keep
+// the fastest.  Results are cached per (grid, precision, device) for the process.
+
+struct TuneKey {
+    int nx, ny, nt, prec, dev;
+    bool operator==(const TuneKey &o) const
+    {
+        return nx == o.nx && ny == o.ny && nt == o.nt && prec == o.prec && dev == o.dev;
+    }
+};
+struct TuneEntry {
+    TuneKey key;
+    opo::PassVariant v[3];
+    size_t te[3];
+};
+std::mutex g_tune_mu;
+std::vector<TuneEntry> g_tune_cache;
+
+template <typename C> int time_pass(OpoSolver *s, int kind, float *ms)
+{
+    const double zh[2] = {0, 0};
+    cudaEvent_t a = nullptr, b = nullptr;
+    OPO_CU(s, cudaEventCreate(&a), "event");
+    OPO_CU(s, cudaEventCreate(&b), "event");
+    int rc = OPO_OK;
+    const int warm = 2, reps = 6;
+    for (int r = 0; r < warm + reps && !rc; r++) {
+        if (r == warm) cudaEventRecord(a, s->stream);
+        rc = kind == kT ? enqueue_t<C>(s, false, 2, zh, 0, 7u) : enqueue_axis<C>(s, kind, 0, 7u);
+    }
+    cudaEventRecord(b, s->stream);
+    cudaError_t e = cudaEventSynchronize(b);
+    float t = 0;
+    if (!rc && e == cudaSuccess) cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(s, e, "autotune timing");
+    *ms = t / reps;
+    return OPO_OK;
+}
+
+template <typename C> int autotune(OpoSolver *s)
+{
+    const bool fp64 = sizeof(C) == 16;
+    const TuneKey key{s->p.nx, s->p.ny, s->p.nt, s->p.precision, s->dev};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        for (auto &e : g_tune_cache)
+            if (e.key == key) {
+                for (int k = 0; k < 3; k++) {
+                    int rc = configure_pass<C>(s, k, e.v[k], e.te[k]);
+                    if (rc) return rc;
+                }
+                return OPO_OK;
+            }
+    }
+    TuneEntry best{key, {}, {}};
+    const size_t tes[2] = {fp64 ? 1024u : 2048u, fp64 ? 2048u : 4096u};
+    const int threads[2] = {128, 256};
+    const int r1s[3] = {4, 8, 16};
+    const long long launches0 = s->launches;
+    for (int kind = 0; kind < 3; kind++) {
+        float best_ms = 1e30f;
+        best.v[kind] = s->pass[kind].v;
+        best.te[kind] = s->pass[kind].te;
+        for (size_t te : tes)
+            for (int th : threads)
+                for (int r1 : r1s) {
+                    if (fp64 && kind == kT && r1 > 8) continue;
+                    if (configure_pass<C>(s, kind, opo::PassVariant{th, r1}, te) != OPO_OK) continue;
+                    if (s->pass[kind].v.r1 != r1) continue;  // plan fell back to a smaller radix
+                    float ms = 0;
+                    int rc = time_pass<C>(s, kind, &ms);
+                    if (rc) return rc;
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best.v[kind] = s->pass[kind].v;
+                        best.te[kind] = te;
+                    }
+                }
+        int rc = configure_pass<C>(s, kind, best.v[kind], best.te[kind]);
+        if (rc) return rc;
+    }
+    s->launches = launches0;
+    // the timed passes ran on the resident fields: leave them zeroed
+    for (int k = 1; k < 4; k++) OPO_CU(s, cudaMemsetAsync(s->field[k], 0, s->esz * s->V, s->stream), "memset");
+    OPO_CU(s, cudaStreamSynchronize(s->stream), "autotune sync");
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache.push_back(best);
     return OPO_OK;
 }
 
@@ -821,18 +940,20 @@ int opo_create(const OpoParams *p, const double *w, OpoSolver **out)
             else if ((e = cudaMemset(s->field[k], 0, s->esz * s->V)) != cudaSuccess) rc = cuda_fail(s, e, "memset");
         }
         if (rc) break;
-        rc = p->precision == OPO_FP64 ? setup_tables<double2>(s) : setup_tables<float2>(s);
-        if (rc) break;
-        size_t mx = s->smem_t;
-        if (s->smem_x > mx) mx = s->smem_x;
-        if (s->smem_y > mx) mx = s->smem_y;
-        if (mx > 227 * 1024) { rc = fail(s, OPO_ERR_INVALID, "tile does not fit in shared memory"); break; }
         // The attribute is per kernel function and shared by every solver of the process:
         // always allow the full 227 KB so no solver lowers it under another.
         if ((e = opo::configure_kernels(227 * 1024)) != cudaSuccess) {
             rc = cuda_fail(s, e, "configure kernels");
             break;
         }
+        for (int k = 0; k < 3 && !rc; k++) {
+            opo::PassVariant v;
+            size_t te;
+            default_variant(p->precision == OPO_FP64, k, v, te);
+            rc = p->precision == OPO_FP64 ? configure_pass<double2>(s, k, v, te) : configure_pass<float2>(s, k, v, te);
+        }
+        if (rc) break;
+        s->gdd_or_mirror = s->p.gdd != 0 || (s->p.resonant & 6u);
         s->sum_blocks = 148 * 4;
         if ((e = cudaMalloc((void **)&s->partials, sizeof(double) * 3 * (s->sum_blocks + 1))) != cudaSuccess) {
             rc = cuda_fail(s, e, "cudaMalloc(partials)");
@@ -861,15 +982,11 @@ void opo_destroy(OpoSolver *s)
         cudaEventDestroy(t.b);
     }
     for (auto e : s->ev_pool) cudaEventDestroy(e);
-    for (auto *pp : s->allocs) cudaFree(pp);
     for (auto *f : s->field)
         if (f) cudaFree(f);
     if (s->partials) cudaFree(s->partials);
     if (s->staging) cudaFree(s->staging);
-    if (s->tables) {
-        if (s->p.precision == OPO_FP64) delete static_cast<Tables<double2> *>(s->tables);
-        else delete static_cast<Tables<float2> *>(s->tables);
-    }
+    for (auto &pc : s->pass) free_pass(pc);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -975,6 +1092,23 @@ int opo_pass_times(OpoSolver *s, double ms[4], long long counts[4])
         s->ev_pool.push_back(t.b);
     }
     s->timed.clear();
+    return OPO_OK;
+}
+
+int opo_autotune(OpoSolver *s)
+{
+    if (!s) return OPO_ERR_INVALID;
+    return s->p.precision == OPO_FP64 ? autotune<double2>(s) : autotune<float2>(s);
+}
+
+int opo_get_tuning(const OpoSolver *s, int out[9])
+{
+    if (!s || !out) return OPO_ERR_INVALID;
+    for (int k = 0; k < 3; k++) {
+        out[3 * k] = s->pass[k].v.threads;
+        out[3 * k + 1] = (int)s->pass[k].te;
+        out[3 * k + 2] = s->pass[k].v.r1;
+    }
     return OPO_OK;
 }
 

@@ -8,7 +8,21 @@
 namespace opo {
 
 constexpr int kMaxStages = 8;
-constexpr int kThreads = 256;        // threads per CTA of every pass kernel
+
+// Division by a run-time invariant d for n < 2^31 with one multiply-high and a shift
+// (Granlund & Montgomery, "Division by invariant integers using multiplication", 1994):
+// q = (m ? umulhi(n, m) : n) >> s, with m = ceil(2^(31+l) / d), s = l - 1, l = ceil(log2 d)
+// for d not a power of two, and m = 0, s = log2 d otherwise.
+struct FastDiv {
+    unsigned d, m, s;
+};
+
+#ifdef __CUDACC__
+__device__ __forceinline__ unsigned fdiv(const FastDiv &f, unsigned n)
+{
+    return (f.m ? __umulhi(n, f.m) : n) >> f.s;
+}
+#endif
 
 // In-place line FFT of length n done in `ns` stages.  Forward stages are decimation in
 // frequency: stage s splits sub-sequences of length len[s] with radix radix[s]
@@ -23,6 +37,7 @@ struct AxisPlan {
     int radix[kMaxStages];
     int len[kMaxStages];
     int twoff[kMaxStages];
+    FastDiv q[kMaxStages];  // len[s] / radix[s]
 };
 
 // Placement of one tile of lines.  Line l, element j of tile `tile` is the global
@@ -33,9 +48,10 @@ struct TileGeom {
     int nlines;
     int LS;
     int ntiles;
-    int tdiv;
-    long long tmulA, tmulB;
-    long long gs_j, gs_l;
+    FastDiv tdiv;
+    FastDiv nl;  // nlines
+    unsigned tmulA, tmulB;
+    unsigned gs_j, gs_l;
 };
 
 template <typename C> struct RealOf;
@@ -63,7 +79,7 @@ template <typename C> struct TPassArgs {
     T c1, c3, h6;       // RK4 stage offsets (k1, k2 -> c1; k3 -> c3) and final weight h/6
     C ph[2][3];         // exp(i dk z) at the stage positions z, z+h/2, z+h of each half step
     int skip_rows;      // shipped quirk: transform only row y = 0 (tiles with y != 0 skip)
-    int nx;             // grid width (for the row test above)
+    unsigned nx;        // grid width (for the row test above)
 };
 
 template <typename C> struct AxisArgs {
@@ -75,10 +91,20 @@ template <typename C> struct AxisArgs {
     unsigned tmask;
 };
 
-// Launchers (ssfm_kernels.cu).  smem in bytes; grid = number of CTAs.
-template <typename C> cudaError_t launch_tpass(const TPassArgs<C> &a, int r1, int grid, size_t smem,
+// Kernel variant of one pass: CTA size and first-stage radix; the largest radix any
+// stage may use follows from the precision and CTA size (max_radix()).
+struct PassVariant {
+    int threads;  // 128 or 256
+    int r1;       // 4, 8 or 16
+};
+
+inline int max_radix(bool fp64, int threads) { return (fp64 && threads == 128) ? 8 : 16; }
+
+// Launchers (ssfm_kernels.cu).  smem in bytes; grid = number of CTAs.  They return
+// cudaErrorInvalidValue for a variant that is not compiled.
+template <typename C> cudaError_t launch_tpass(const TPassArgs<C> &a, PassVariant v, int grid, size_t smem,
                                                cudaStream_t st);
-template <typename C> cudaError_t launch_axis(const AxisArgs<C> &a, int r1, bool bfast, int grid,
+template <typename C> cudaError_t launch_axis(const AxisArgs<C> &a, PassVariant v, bool bfast, int grid,
                                               size_t smem, cudaStream_t st);
 template <typename C> cudaError_t launch_sums(const C *f0, const C *f1, const C *f2, size_t n,
                                               double *partials, int nblocks, double *out,

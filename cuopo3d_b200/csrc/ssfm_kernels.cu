@@ -13,6 +13,9 @@
 // t-pass, with the RK4 update) and the last inverse stage with the global store.  The
 // middle stages exchange through shared memory; the last forward stage, the phase
 // multiply and the first inverse stage are one register-resident step.
+//
+// Index arithmetic is 32-bit (a field holds fewer than 2^32 values) and every division
+// by a run-time invariant uses a precomputed multiply-high (FastDiv).
 
 #include "fft_radix.cuh"
 #include "opo_internal.h"
@@ -32,112 +35,130 @@ __device__ __forceinline__ float2 tab_mul(float2 x, float4 t)
     return make_float2(a.x + b.x, a.y + b.y);
 }
 
-__device__ __forceinline__ long long tile_base(const TileGeom &g, int tile)
+__device__ __forceinline__ unsigned tile_base(const TileGeom &g, unsigned tile)
 {
-    return (long long)(tile % g.tdiv) * g.tmulA + (long long)(tile / g.tdiv) * g.tmulB;
+    const unsigned hi = fdiv(g.tdiv, tile);
+    return (tile - hi * g.tdiv.d) * g.tmulA + hi * g.tmulB;
+}
+
+// Index of the f-th field (in p, s, i order) selected by mask.
+__device__ __forceinline__ int field_id(unsigned mask, int f)
+{
+    for (int k = 0; k < 3; k++)
+        if (mask & (1u << k)) {
+            if (f == 0) return k;
+            f--;
+        }
+    return 0;
 }
 
 // ---------------------------------------------------------------------------------
-// Shared-memory stages.  Work item w -> (line l fastest, butterfly b, field slot f).
+// Shared-memory stages.  Per field, work item w -> (line l fastest, butterfly b).
 
-template <typename C, int R, int S, bool DIT>
-__device__ void smem_stage(C *sm, int LS, int nlines, int n, int L, const C *tw, int nf,
-                           const int *fslot)
+template <typename C, int R, int S, bool DIT, int THREADS>
+__device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv &fq, const C *tw, int nf)
 {
-    const int q = L / R, nb = n / R;
-    const int per_field = nb * nlines;
-    for (int w = threadIdx.x; w < per_field * nf; w += blockDim.x) {
-        const int f = w / per_field, r = w - f * per_field;
-        const int b = r / nlines, l = r - b * nlines;
-        const int g = b / q, j = b - g * q, base = g * L + j;
-        C *s = sm + (size_t)fslot[f] * n * LS + l;
-        C x[R];
+    const unsigned q = fq.d, nl = (unsigned)g.nlines, LS = (unsigned)g.LS;
+    const unsigned items = (unsigned)(n / R) * nl;
+    for (int f = 0; f < nf; f++) {
+        C *sf = sm + (size_t)f * n * LS;
+        for (unsigned w = threadIdx.x; w < items; w += THREADS) {
+            const unsigned b = fdiv(g.nl, w), l = w - b * nl;
+            const unsigned gq = fdiv(fq, b), j = b - gq * q;
+            C *s = sf + (gq * L + j) * LS + l;
+            C x[R];
 #pragma unroll
-        for (int m = 0; m < R; m++) x[m] = s[(base + m * q) * LS];
-        if (DIT && q > 1) {
+            for (int m = 0; m < R; m++) x[m] = s[m * q * LS];
+            if (DIT && q > 1) {
 #pragma unroll
-            for (int m = 1; m < R; m++) x[m] = twmul<S>(x[m], __ldg(tw + (m - 1) * q + j));
+                for (int m = 1; m < R; m++) x[m] = twmul<S>(x[m], __ldg(tw + (m - 1) * q + j));
+            }
+            dft<R, S>(x);
+            if (!DIT && q > 1) {
+#pragma unroll
+                for (int k = 1; k < R; k++) x[k] = twmul<S>(x[k], __ldg(tw + (k - 1) * q + j));
+            }
+#pragma unroll
+            for (int k = 0; k < R; k++) s[k * q * LS] = x[k];
         }
-        dft<R, S>(x);
-        if (!DIT && q > 1) {
-#pragma unroll
-            for (int k = 1; k < R; k++) x[k] = twmul<S>(x[k], __ldg(tw + (k - 1) * q + j));
-        }
-#pragma unroll
-        for (int k = 0; k < R; k++) s[(base + k * q) * LS] = x[k];
     }
 }
 
 // Last forward stage (q = 1), phase multiply, first inverse stage, in registers.
-template <typename C, int R, int SF>
-__device__ void fused_middle(C *sm, int LS, int nlines, int n, const typename TabOf<C>::type *const *tab,
-                             int nf, const int *fslot, const int *fid)
+template <typename C, int R, int SF, int THREADS>
+__device__ void fused_middle(C *sm, const TileGeom &g, int n, const typename TabOf<C>::type *const *tab,
+                             unsigned tmask, int nf)
 {
-    const int nb = n / R;
-    const int per_field = nb * nlines;
-    for (int w = threadIdx.x; w < per_field * nf; w += blockDim.x) {
-        const int f = w / per_field, r = w - f * per_field;
-        const int g = r / nlines, l = r - g * nlines;
-        C *s = sm + (size_t)fslot[f] * n * LS + l;
-        const typename TabOf<C>::type *tb = tab[fid[f]] + g * R;
-        C x[R];
+    const unsigned nl = (unsigned)g.nlines, LS = (unsigned)g.LS;
+    const unsigned items = (unsigned)(n / R) * nl;
+    for (int f = 0; f < nf; f++) {
+        C *sf = sm + (size_t)f * n * LS;
+        const typename TabOf<C>::type *tf = tab[field_id(tmask, f)];
+        for (unsigned w = threadIdx.x; w < items; w += THREADS) {
+            const unsigned g0 = fdiv(g.nl, w), l = w - g0 * nl;
+            C *s = sf + g0 * R * LS + l;
+            const typename TabOf<C>::type *tb = tf + g0 * R;
+            C x[R];
 #pragma unroll
-        for (int m = 0; m < R; m++) x[m] = s[(g * R + m) * LS];
-        dft<R, SF>(x);
+            for (int m = 0; m < R; m++) x[m] = s[m * LS];
+            dft<R, SF>(x);
 #pragma unroll
-        for (int k = 0; k < R; k++) x[k] = tab_mul(x[k], __ldg(tb + k));
-        dft<R, -SF>(x);
+            for (int k = 0; k < R; k++) x[k] = tab_mul(x[k], __ldg(tb + k));
+            dft<R, -SF>(x);
 #pragma unroll
-        for (int k = 0; k < R; k++) s[(g * R + k) * LS] = x[k];
+            for (int k = 0; k < R; k++) s[k * LS] = x[k];
+        }
     }
 }
 
-template <typename C, int S, bool DIT>
-__device__ void smem_stage_dispatch(int R, C *sm, int LS, int nlines, int n, int L, const C *tw,
-                                    int nf, const int *fslot)
+template <typename C, int S, bool DIT, int THREADS, int RMAX>
+__device__ void smem_stage_dispatch(int R, C *sm, const TileGeom &g, int n, int L, const FastDiv &fq,
+                                    const C *tw, int nf)
 {
     switch (R) {
-    case 2: smem_stage<C, 2, S, DIT>(sm, LS, nlines, n, L, tw, nf, fslot); break;
-    case 3: smem_stage<C, 3, S, DIT>(sm, LS, nlines, n, L, tw, nf, fslot); break;
-    case 4: smem_stage<C, 4, S, DIT>(sm, LS, nlines, n, L, tw, nf, fslot); break;
-    case 8: smem_stage<C, 8, S, DIT>(sm, LS, nlines, n, L, tw, nf, fslot); break;
-    case 16: smem_stage<C, 16, S, DIT>(sm, LS, nlines, n, L, tw, nf, fslot); break;
+    case 2: smem_stage<C, 2, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf); break;
+    case 3: smem_stage<C, 3, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf); break;
+    case 4: smem_stage<C, 4, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf); break;
+    case 8: smem_stage<C, 8, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf); break;
+    case 16:
+        if constexpr (RMAX >= 16) smem_stage<C, 16, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf);
+        break;
     default: break;
     }
 }
 
-template <typename C, int SF>
-__device__ void fused_dispatch(int R, C *sm, int LS, int nlines, int n,
-                               const typename TabOf<C>::type *const *tab, int nf, const int *fslot,
-                               const int *fid)
+template <typename C, int SF, int THREADS, int RMAX>
+__device__ void fused_dispatch(int R, C *sm, const TileGeom &g, int n, const typename TabOf<C>::type *const *tab,
+                               unsigned tmask, int nf)
 {
     switch (R) {
-    case 2: fused_middle<C, 2, SF>(sm, LS, nlines, n, tab, nf, fslot, fid); break;
-    case 3: fused_middle<C, 3, SF>(sm, LS, nlines, n, tab, nf, fslot, fid); break;
-    case 4: fused_middle<C, 4, SF>(sm, LS, nlines, n, tab, nf, fslot, fid); break;
-    case 8: fused_middle<C, 8, SF>(sm, LS, nlines, n, tab, nf, fslot, fid); break;
-    case 16: fused_middle<C, 16, SF>(sm, LS, nlines, n, tab, nf, fslot, fid); break;
+    case 2: fused_middle<C, 2, SF, THREADS>(sm, g, n, tab, tmask, nf); break;
+    case 3: fused_middle<C, 3, SF, THREADS>(sm, g, n, tab, tmask, nf); break;
+    case 4: fused_middle<C, 4, SF, THREADS>(sm, g, n, tab, tmask, nf); break;
+    case 8: fused_middle<C, 8, SF, THREADS>(sm, g, n, tab, tmask, nf); break;
+    case 16:
+        if constexpr (RMAX >= 16) fused_middle<C, 16, SF, THREADS>(sm, g, n, tab, tmask, nf);
+        break;
     default: break;
     }
 }
 
 // Stages 1 .. ns-1 forward, fused middle, inverse back to stage 1 (stage 0 is fused
 // with the global load / store by the caller).
-template <typename C, int SF>
+template <typename C, int SF, int THREADS, int RMAX>
 __device__ void middle_stages(C *sm, const TileGeom &g, const AxisPlan &p, const C *tw,
-                              const typename TabOf<C>::type *const *tab, int nf, const int *fslot,
-                              const int *fid)
+                              const typename TabOf<C>::type *const *tab, unsigned tmask, int nf)
 {
     for (int s = 1; s < p.ns - 1; s++) {
-        smem_stage_dispatch<C, SF, false>(p.radix[s], sm, g.LS, g.nlines, p.n, p.len[s],
-                                          tw + p.twoff[s], nf, fslot);
+        smem_stage_dispatch<C, SF, false, THREADS, RMAX>(p.radix[s], sm, g, p.n, p.len[s], p.q[s],
+                                                         tw + p.twoff[s], nf);
         __syncthreads();
     }
-    fused_dispatch<C, SF>(p.radix[p.ns - 1], sm, g.LS, g.nlines, p.n, tab, nf, fslot, fid);
+    fused_dispatch<C, SF, THREADS, RMAX>(p.radix[p.ns - 1], sm, g, p.n, tab, tmask, nf);
     __syncthreads();
     for (int s = p.ns - 2; s >= 1; s--) {
-        smem_stage_dispatch<C, -SF, true>(p.radix[s], sm, g.LS, g.nlines, p.n, p.len[s],
-                                          tw + p.twoff[s], nf, fslot);
+        smem_stage_dispatch<C, -SF, true, THREADS, RMAX>(p.radix[s], sm, g, p.n, p.len[s], p.q[s],
+                                                         tw + p.twoff[s], nf);
         __syncthreads();
     }
 }
@@ -210,29 +231,28 @@ __device__ __forceinline__ void rk4_half(const TPassArgs<C> &a, int h, C &p, C &
 // for p, s, i, applies n_rk4 half steps to each voxel, then the first forward stage of
 // every transformed field into shared memory (untransformed fields go straight back).
 
-template <typename C, int R1>
-__global__ void __launch_bounds__(kThreads) tpass_kernel(TPassArgs<C> a)
+template <typename C, int R1, int THREADS, int RMAX>
+__global__ void __launch_bounds__(THREADS, THREADS == 128 ? 4 : 1) tpass_kernel(TPassArgs<C> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *sm = reinterpret_cast<C *>(smem_raw);
     const AxisPlan &p = a.plan;
     const TileGeom &g = a.g;
-    const int n = p.n, q = n / R1, P = g.nlines, LS = g.LS;
-    int fslot[3], fid[3], nf = 0;
-    for (int f = 0; f < 3; f++)
-        if (a.tmask & (1u << f)) { fslot[nf] = nf; fid[nf] = f; nf++; }
+    const unsigned n = p.n, q = n / R1, P = g.nlines, LS = g.LS;
+    const int nf = __popc(a.tmask);
 
-    for (int tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
-        const long long base = tile_base(g, tile);
+    for (unsigned tile = blockIdx.x; tile < (unsigned)g.ntiles; tile += gridDim.x) {
+        const unsigned base = tile_base(g, tile);
         bool xform = nf > 0;
-        if (a.skip_rows && (base / a.nx) % (g.gs_j / a.nx) != 0) xform = false;
-        for (int w = threadIdx.x; w < q * P; w += blockDim.x) {
-            const int b = w / P, l = w - b * P;
-            const long long gb = base + (long long)l * g.gs_l + (long long)b * g.gs_j;
+        if (a.skip_rows && base >= a.nx) xform = false;  // row y = base / nx != 0
+        for (unsigned w = threadIdx.x; w < q * P; w += THREADS) {
+            const unsigned b = fdiv(g.nl, w), l = w - b * P;
+            const unsigned gb = base + l * g.gs_l + b * g.gs_j;
+            const unsigned gstep = q * g.gs_j;
             C x[3][R1];
 #pragma unroll
             for (int m = 0; m < R1; m++) {
-                const long long gi = gb + (long long)m * q * g.gs_j;
+                const unsigned gi = gb + m * gstep;
                 x[0][m] = a.psrc[gi];
                 x[1][m] = a.f[1][gi];
                 x[2][m] = a.f[2][gi];
@@ -241,40 +261,41 @@ __global__ void __launch_bounds__(kThreads) tpass_kernel(TPassArgs<C> a)
 #pragma unroll
                 for (int m = 0; m < R1; m++) rk4_half(a, h, x[0][m], x[1][m], x[2][m]);
             }
-            int slot = 0;
 #pragma unroll
             for (int f = 0; f < 3; f++) {
                 if (xform && (a.tmask & (1u << f))) {
                     dft<R1, +1>(x[f]);
 #pragma unroll
                     for (int k = 1; k < R1; k++) x[f][k] = twmul<+1>(x[f][k], __ldg(a.tw + (k - 1) * q + b));
-                    C *s = sm + (size_t)slot * n * LS + l;
+                    C *s = sm + (size_t)__popc(a.tmask & ((1u << f) - 1u)) * n * LS + b * LS + l;
 #pragma unroll
-                    for (int k = 0; k < R1; k++) s[(b + k * q) * LS] = x[f][k];
-                    slot++;
+                    for (int k = 0; k < R1; k++) s[k * q * LS] = x[f][k];
                 } else {
 #pragma unroll
-                    for (int m = 0; m < R1; m++) a.f[f][gb + (long long)m * q * g.gs_j] = x[f][m];
+                    for (int m = 0; m < R1; m++) a.f[f][gb + m * gstep] = x[f][m];
                 }
             }
         }
         if (!xform) continue;
         __syncthreads();
-        middle_stages<C, +1>(sm, g, p, a.tw, a.tab, nf, fslot, fid);
+        middle_stages<C, +1, THREADS, RMAX>(sm, g, p, a.tw, a.tab, a.tmask, nf);
         // Stage 0 inverse (sign -1) and store.
-        for (int w = threadIdx.x; w < q * P * nf; w += blockDim.x) {
-            const int f = w / (q * P), r = w - f * (q * P);
-            const int b = r / P, l = r - b * P;
-            C *s = sm + (size_t)fslot[f] * n * LS + l;
-            C x[R1];
+        for (int f = 0; f < nf; f++) {
+            C *sf = sm + (size_t)f * n * LS;
+            C *dstf = a.f[field_id(a.tmask, f)];
+            for (unsigned w = threadIdx.x; w < q * P; w += THREADS) {
+                const unsigned b = fdiv(g.nl, w), l = w - b * P;
+                const C *s = sf + b * LS + l;
+                C x[R1];
 #pragma unroll
-            for (int m = 0; m < R1; m++) x[m] = s[(b + m * q) * LS];
+                for (int m = 0; m < R1; m++) x[m] = s[m * q * LS];
 #pragma unroll
-            for (int m = 1; m < R1; m++) x[m] = twmul<-1>(x[m], __ldg(a.tw + (m - 1) * q + b));
-            dft<R1, -1>(x);
-            C *dst = a.f[fid[f]] + base + (long long)l * g.gs_l + (long long)b * g.gs_j;
+                for (int m = 1; m < R1; m++) x[m] = twmul<-1>(x[m], __ldg(a.tw + (m - 1) * q + b));
+                dft<R1, -1>(x);
+                C *dst = dstf + base + l * g.gs_l + b * g.gs_j;
 #pragma unroll
-            for (int k = 0; k < R1; k++) dst[(long long)k * q * g.gs_j] = x[k];
+                for (int k = 0; k < R1; k++) dst[k * q * g.gs_j] = x[k];
+            }
         }
         __syncthreads();
     }
@@ -286,70 +307,69 @@ __global__ void __launch_bounds__(kThreads) tpass_kernel(TPassArgs<C> a)
 // consecutive butterflies of a line (x axis, where lines are rows and the transform
 // index is the contiguous one); otherwise consecutive threads take consecutive lines.
 
-template <typename C, int R1, bool BFAST>
-__global__ void __launch_bounds__(kThreads) axis_kernel(AxisArgs<C> a)
+template <bool BFAST>
+__device__ __forceinline__ void axis_item(unsigned w, const FastDiv &fq, const FastDiv &fnl, unsigned &b,
+                                          unsigned &l)
+{
+    if (BFAST) {
+        l = fdiv(fq, w);
+        b = w - l * fq.d;
+    } else {
+        b = fdiv(fnl, w);
+        l = w - b * fnl.d;
+    }
+}
+
+template <typename C, int R1, bool BFAST, int THREADS, int RMAX>
+__global__ void __launch_bounds__(THREADS, THREADS == 128 ? 4 : 1) axis_kernel(AxisArgs<C> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *sm = reinterpret_cast<C *>(smem_raw);
     const AxisPlan &p = a.plan;
     const TileGeom &g = a.g;
-    const int n = p.n, q = n / R1, NL = g.nlines, LS = g.LS;
-    int fslot[3], fid[3], nf = 0;
-    for (int f = 0; f < 3; f++)
-        if (a.tmask & (1u << f)) { fslot[nf] = nf; fid[nf] = f; nf++; }
-    const int items = q * NL * nf;
+    const unsigned n = p.n, q = n / R1, NL = g.nlines, LS = g.LS;
+    const int nf = __popc(a.tmask);
+    const unsigned items = q * NL;
 
-    for (int tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
-        const long long base = tile_base(g, tile);
-        for (int w = threadIdx.x; w < items; w += blockDim.x) {
-            int f, b, l;
-            if (BFAST) {
-                b = w % q;
-                const int r = w / q;
-                l = r % NL;
-                f = r / NL;
-            } else {
-                l = w % NL;
-                const int r = w / NL;
-                b = r % q;
-                f = r / q;
+    for (unsigned tile = blockIdx.x; tile < (unsigned)g.ntiles; tile += gridDim.x) {
+        const unsigned base = tile_base(g, tile);
+        for (int f = 0; f < nf; f++) {
+            const C *srcf = a.f[field_id(a.tmask, f)] + base;
+            C *sf = sm + (size_t)f * n * LS;
+            for (unsigned w = threadIdx.x; w < items; w += THREADS) {
+                unsigned b, l;
+                axis_item<BFAST>(w, p.q[0], g.nl, b, l);
+                const C *src = srcf + l * g.gs_l + b * g.gs_j;
+                C x[R1];
+#pragma unroll
+                for (int m = 0; m < R1; m++) x[m] = src[m * q * g.gs_j];
+                dft<R1, -1>(x);
+#pragma unroll
+                for (int k = 1; k < R1; k++) x[k] = twmul<-1>(x[k], __ldg(a.tw + (k - 1) * q + b));
+                C *s = sf + b * LS + l;
+#pragma unroll
+                for (int k = 0; k < R1; k++) s[k * q * LS] = x[k];
             }
-            const C *src = a.f[fid[f]] + base + (long long)l * g.gs_l + (long long)b * g.gs_j;
-            C x[R1];
-#pragma unroll
-            for (int m = 0; m < R1; m++) x[m] = src[(long long)m * q * g.gs_j];
-            dft<R1, -1>(x);
-#pragma unroll
-            for (int k = 1; k < R1; k++) x[k] = twmul<-1>(x[k], __ldg(a.tw + (k - 1) * q + b));
-            C *s = sm + (size_t)fslot[f] * n * LS + l;
-#pragma unroll
-            for (int k = 0; k < R1; k++) s[(b + k * q) * LS] = x[k];
         }
         __syncthreads();
-        middle_stages<C, -1>(sm, g, p, a.tw, a.tab, nf, fslot, fid);
-        for (int w = threadIdx.x; w < items; w += blockDim.x) {
-            int f, b, l;
-            if (BFAST) {
-                b = w % q;
-                const int r = w / q;
-                l = r % NL;
-                f = r / NL;
-            } else {
-                l = w % NL;
-                const int r = w / NL;
-                b = r % q;
-                f = r / q;
+        middle_stages<C, -1, THREADS, RMAX>(sm, g, p, a.tw, a.tab, a.tmask, nf);
+        for (int f = 0; f < nf; f++) {
+            C *dstf = a.f[field_id(a.tmask, f)] + base;
+            const C *sf = sm + (size_t)f * n * LS;
+            for (unsigned w = threadIdx.x; w < items; w += THREADS) {
+                unsigned b, l;
+                axis_item<BFAST>(w, p.q[0], g.nl, b, l);
+                const C *s = sf + b * LS + l;
+                C x[R1];
+#pragma unroll
+                for (int m = 0; m < R1; m++) x[m] = s[m * q * LS];
+#pragma unroll
+                for (int m = 1; m < R1; m++) x[m] = twmul<+1>(x[m], __ldg(a.tw + (m - 1) * q + b));
+                dft<R1, +1>(x);
+                C *dst = dstf + l * g.gs_l + b * g.gs_j;
+#pragma unroll
+                for (int k = 0; k < R1; k++) dst[k * q * g.gs_j] = x[k];
             }
-            C *s = sm + (size_t)fslot[f] * n * LS + l;
-            C x[R1];
-#pragma unroll
-            for (int m = 0; m < R1; m++) x[m] = s[(b + m * q) * LS];
-#pragma unroll
-            for (int m = 1; m < R1; m++) x[m] = twmul<+1>(x[m], __ldg(a.tw + (m - 1) * q + b));
-            dft<R1, +1>(x);
-            C *dst = a.f[fid[f]] + base + (long long)l * g.gs_l + (long long)b * g.gs_j;
-#pragma unroll
-            for (int k = 0; k < R1; k++) dst[(long long)k * q * g.gs_j] = x[k];
         }
         __syncthreads();
     }
@@ -359,11 +379,13 @@ __global__ void __launch_bounds__(kThreads) axis_kernel(AxisArgs<C> a)
 // FP64 sums of |A|^2 for three fields: per-block partials, then one block adds the
 // partials in a fixed order (deterministic).
 
+constexpr int kSumThreads = 256;
+
 template <typename C>
-__global__ void __launch_bounds__(kThreads) sums_partial_kernel(const C *f0, const C *f1, const C *f2,
-                                                                 size_t n, double *partials)
+__global__ void __launch_bounds__(kSumThreads) sums_partial_kernel(const C *f0, const C *f1, const C *f2,
+                                                                    size_t n, double *partials)
 {
-    __shared__ double red[3][kThreads / 32];
+    __shared__ double red[3][kSumThreads / 32];
     double acc[3] = {0, 0, 0};
     const C *fs[3] = {f0, f1, f2};
     for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (size_t)gridDim.x * blockDim.x) {
@@ -382,7 +404,7 @@ __global__ void __launch_bounds__(kThreads) sums_partial_kernel(const C *f0, con
     __syncthreads();
     if (threadIdx.x < 3) {
         double v = 0;
-        for (int wv = 0; wv < kThreads / 32; wv++) v += red[threadIdx.x][wv];
+        for (int wv = 0; wv < kSumThreads / 32; wv++) v += red[threadIdx.x][wv];
         partials[(size_t)blockIdx.x * 3 + threadIdx.x] = v;
     }
 }
@@ -409,107 +431,101 @@ __global__ void convert_f2d_kernel(const float2 *src, double2 *dst, size_t n)
 }
 
 // ---------------------------------------------------------------------------------
-// Launchers.
+// Compiled variants: (element type, threads, first-stage radix, largest radix).
 
-template <typename C, int R1> static cudaError_t set_attr_t(size_t smem)
-{
-    return cudaFuncSetAttribute(tpass_kernel<C, R1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-}
-template <typename C, int R1, bool B> static cudaError_t set_attr_a(size_t smem)
-{
-    return cudaFuncSetAttribute(axis_kernel<C, R1, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-}
+#define OPO_T_VARIANTS(X)                                                                          \
+    X(float2, 128, 4, 16) X(float2, 128, 8, 16) X(float2, 128, 16, 16) X(float2, 256, 4, 16)        \
+    X(float2, 256, 8, 16) X(float2, 256, 16, 16) X(double2, 128, 4, 8) X(double2, 128, 8, 8)        \
+    X(double2, 256, 4, 16) X(double2, 256, 8, 16)
+
+#define OPO_A_VARIANTS(X)                                                                          \
+    X(float2, 128, 4, 16) X(float2, 128, 8, 16) X(float2, 128, 16, 16) X(float2, 256, 4, 16)        \
+    X(float2, 256, 8, 16) X(float2, 256, 16, 16) X(double2, 128, 4, 8) X(double2, 128, 8, 8)        \
+    X(double2, 256, 4, 16) X(double2, 256, 8, 16) X(double2, 256, 16, 16)
 
 cudaError_t configure_kernels(size_t smem)
 {
-    cudaError_t e = cudaSuccess;
-#define OPO_ATTR(expr) \
-    if ((e = (expr)) != cudaSuccess) return e;
-    OPO_ATTR((set_attr_t<float2, 4>(smem)));
-    OPO_ATTR((set_attr_t<float2, 8>(smem)));
-    OPO_ATTR((set_attr_t<float2, 16>(smem)));
-    OPO_ATTR((set_attr_t<double2, 4>(smem)));
-    OPO_ATTR((set_attr_t<double2, 8>(smem)));
-    OPO_ATTR((set_attr_a<float2, 4, true>(smem)));
-    OPO_ATTR((set_attr_a<float2, 8, true>(smem)));
-    OPO_ATTR((set_attr_a<float2, 16, true>(smem)));
-    OPO_ATTR((set_attr_a<float2, 4, false>(smem)));
-    OPO_ATTR((set_attr_a<float2, 8, false>(smem)));
-    OPO_ATTR((set_attr_a<float2, 16, false>(smem)));
-    OPO_ATTR((set_attr_a<double2, 4, true>(smem)));
-    OPO_ATTR((set_attr_a<double2, 8, true>(smem)));
-    OPO_ATTR((set_attr_a<double2, 16, true>(smem)));
-    OPO_ATTR((set_attr_a<double2, 4, false>(smem)));
-    OPO_ATTR((set_attr_a<double2, 8, false>(smem)));
-    OPO_ATTR((set_attr_a<double2, 16, false>(smem)));
-#undef OPO_ATTR
-    return e;
+    cudaError_t e;
+#define OPO_SET_T(C, T, R, RM)                                                                      \
+    if ((e = cudaFuncSetAttribute(tpass_kernel<C, R, T, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                  (int)smem)) != cudaSuccess)                                       \
+        return e;
+#define OPO_SET_A(C, T, R, RM)                                                                      \
+    if ((e = cudaFuncSetAttribute(axis_kernel<C, R, true, T, RM>,                                   \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) \
+        return e;                                                                                   \
+    if ((e = cudaFuncSetAttribute(axis_kernel<C, R, false, T, RM>,                                  \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) \
+        return e;
+    OPO_T_VARIANTS(OPO_SET_T)
+    OPO_A_VARIANTS(OPO_SET_A)
+#undef OPO_SET_T
+#undef OPO_SET_A
+    return cudaSuccess;
 }
 
 template <typename C>
-cudaError_t launch_tpass(const TPassArgs<C> &a, int r1, int grid, size_t smem, cudaStream_t st)
+cudaError_t launch_tpass(const TPassArgs<C> &a, PassVariant v, int grid, size_t smem, cudaStream_t st)
 {
-    switch (r1) {
-    case 4: tpass_kernel<C, 4><<<grid, kThreads, smem, st>>>(a); break;
-    case 8: tpass_kernel<C, 8><<<grid, kThreads, smem, st>>>(a); break;
-    case 16:
-        if constexpr (sizeof(C) == 8) {
-            tpass_kernel<C, 16><<<grid, kThreads, smem, st>>>(a);
-            break;
-        }
-        return cudaErrorInvalidValue;
-    default: return cudaErrorInvalidValue;
+    bool done = false;
+#define OPO_LAUNCH_T(CC, T, R, RM)                                                                  \
+    if constexpr (std::is_same<C, CC>::value) {                                                     \
+        if (!done && v.threads == T && v.r1 == R) {                                                 \
+            tpass_kernel<CC, R, T, RM><<<grid, T, smem, st>>>(a);                                   \
+            done = true;                                                                            \
+        }                                                                                           \
     }
-    return cudaGetLastError();
+    OPO_T_VARIANTS(OPO_LAUNCH_T)
+#undef OPO_LAUNCH_T
+    return done ? cudaGetLastError() : cudaErrorInvalidValue;
 }
 
 template <typename C>
-cudaError_t launch_axis(const AxisArgs<C> &a, int r1, bool bfast, int grid, size_t smem, cudaStream_t st)
+cudaError_t launch_axis(const AxisArgs<C> &a, PassVariant v, bool bfast, int grid, size_t smem, cudaStream_t st)
 {
-#define OPO_AX(R)                                                           \
-    case R:                                                                 \
-        if (bfast) axis_kernel<C, R, true><<<grid, kThreads, smem, st>>>(a);  \
-        else axis_kernel<C, R, false><<<grid, kThreads, smem, st>>>(a);       \
-        break;
-    switch (r1) {
-        OPO_AX(4)
-        OPO_AX(8)
-        OPO_AX(16)
-    default: return cudaErrorInvalidValue;
+    bool done = false;
+#define OPO_LAUNCH_A(CC, T, R, RM)                                                                  \
+    if constexpr (std::is_same<C, CC>::value) {                                                     \
+        if (!done && v.threads == T && v.r1 == R) {                                                 \
+            if (bfast) axis_kernel<CC, R, true, T, RM><<<grid, T, smem, st>>>(a);                   \
+            else axis_kernel<CC, R, false, T, RM><<<grid, T, smem, st>>>(a);                        \
+            done = true;                                                                            \
+        }                                                                                           \
     }
-#undef OPO_AX
-    return cudaGetLastError();
+    OPO_A_VARIANTS(OPO_LAUNCH_A)
+#undef OPO_LAUNCH_A
+    return done ? cudaGetLastError() : cudaErrorInvalidValue;
 }
 
 template <typename C>
 cudaError_t launch_sums(const C *f0, const C *f1, const C *f2, size_t n, double *partials, int nblocks,
                         double *out, cudaStream_t st)
 {
-    sums_partial_kernel<C><<<nblocks, kThreads, 0, st>>>(f0, f1, f2, n, partials);
+    sums_partial_kernel<C><<<nblocks, kSumThreads, 0, st>>>(f0, f1, f2, n, partials);
     sums_final_kernel<<<1, 32, 0, st>>>(partials, nblocks, out);
     return cudaGetLastError();
 }
 
 cudaError_t launch_convert_d2f(const double2 *src, float2 *dst, size_t n, cudaStream_t st)
 {
-    int blocks = (int)((n + kThreads - 1) / kThreads);
+    int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    convert_d2f_kernel<<<blocks, kThreads, 0, st>>>(src, dst, n);
+    convert_d2f_kernel<<<blocks, 256, 0, st>>>(src, dst, n);
     return cudaGetLastError();
 }
 
 cudaError_t launch_convert_f2d(const float2 *src, double2 *dst, size_t n, cudaStream_t st)
 {
-    int blocks = (int)((n + kThreads - 1) / kThreads);
+    int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    convert_f2d_kernel<<<blocks, kThreads, 0, st>>>(src, dst, n);
+    convert_f2d_kernel<<<blocks, 256, 0, st>>>(src, dst, n);
     return cudaGetLastError();
 }
 
-template cudaError_t launch_tpass<float2>(const TPassArgs<float2> &, int, int, size_t, cudaStream_t);
-template cudaError_t launch_tpass<double2>(const TPassArgs<double2> &, int, int, size_t, cudaStream_t);
-template cudaError_t launch_axis<float2>(const AxisArgs<float2> &, int, bool, int, size_t, cudaStream_t);
-template cudaError_t launch_axis<double2>(const AxisArgs<double2> &, int, bool, int, size_t, cudaStream_t);
+template cudaError_t launch_tpass<float2>(const TPassArgs<float2> &, PassVariant, int, size_t, cudaStream_t);
+template cudaError_t launch_tpass<double2>(const TPassArgs<double2> &, PassVariant, int, size_t, cudaStream_t);
+template cudaError_t launch_axis<float2>(const AxisArgs<float2> &, PassVariant, bool, int, size_t, cudaStream_t);
+template cudaError_t launch_axis<double2>(const AxisArgs<double2> &, PassVariant, bool, int, size_t, cudaStream_t);
 template cudaError_t launch_sums<float2>(const float2 *, const float2 *, const float2 *, size_t, double *, int,
                                          double *, cudaStream_t);
 template cudaError_t launch_sums<double2>(const double2 *, const double2 *, const double2 *, size_t, double *,

@@ -178,6 +178,18 @@ int opo_field_sums(OpoSolver *s, double sums[3]);
 int opo_set_pass_timing(OpoSolver *s, int enable);
 int opo_pass_times(OpoSolver *s, double ms[4], long long counts[4]);
 
+/* Time every compiled kernel variant (CTA size, first-stage radix) and tile size of
+ * the t-, x- and y-passes on this solver's grid and keep the fastest for each; results
+ * are cached per (grid, precision, device) for the process, so later solvers of the same
+ * shape reuse them without timing.  The timed passes run on the resident pump, signal
+ * and idler, which are left zeroed: call it right after opo_create.  Stands in for the
+ * reference's compile-time block sizes (DtypesConsts.cuh:48-50). */
+int opo_autotune(OpoSolver *s);
+
+/* Chosen configuration: for the t-, x- and y-pass in turn, {CTA threads, tile elements
+ * per field, first-stage radix}.  No counterpart in the reference. */
+int opo_get_tuning(const OpoSolver *s, int out[9]);
+
 /* The CUDA stream (a cudaStream_t, returned as void*) on which this solver enqueues all
  * of its work, so that callers can order their own work or record timing events on it.
  * No counterpart in the reference (which runs on the legacy default stream). */
