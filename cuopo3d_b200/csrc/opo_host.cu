@@ -369,6 +369,7 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     const OpoParams &p = s->p;
     const bool fp64 = sizeof(C) == 16;
     using TT = typename opo::TabOf<C>::type;
+    if (!opo::variant_compiled(fp64, kind == kT, v)) return fail(s, OPO_ERR_INVALID, "kernel variant not compiled");
     PassCfg pc;
     pc.v = v;
     pc.te = te;
@@ -503,6 +504,11 @@ int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, int wh
     a.c1 = (T)(phys ? 0.5 * h : 0.5);
     a.c3 = (T)(phys ? h : 1.0);
     a.h6 = (T)(h / 6.0);
+    for (int f = 0; f < 3; f++) {
+        a.c1k[f] = (T)((phys ? 0.5 * h : 0.5) * p.kappa[f]);
+        a.c3k[f] = (T)((phys ? h : 1.0) * p.kappa[f]);
+        a.h6k[f] = (T)(h / 6.0 * p.kappa[f]);
+    }
     a.use_phase = phys && p.dk != 0;
     for (int k = 0; k < n_rk4 && k < 2; k++) {
         // stage positions z, z + h/2, z + h (Solver3D.cuh:911-929 pass z, z+dz/4, z+dz/2)
@@ -725,7 +731,7 @@ template <typename C> int autotune(OpoSolver *s)
         for (size_t te : tes)
             for (int th : threads)
                 for (int r1 : r1s) {
-                    if (fp64 && kind == kT && r1 > 8) continue;
+                    if (!opo::variant_compiled(fp64, kind == kT, opo::PassVariant{th, r1})) continue;
                     if (configure_pass<C>(s, kind, opo::PassVariant{th, r1}, te) != OPO_OK) continue;
                     if (s->pass[kind].v.r1 != r1) continue;  // plan fell back to a smaller radix
                     float ms = 0;

@@ -77,6 +77,7 @@ template <typename C> struct TPassArgs {
     int use_phase;      // apply exp(-/+ i dk z) (corrected physics)
     T kappa[3];
     T c1, c3, h6;       // RK4 stage offsets (k1, k2 -> c1; k3 -> c3) and final weight h/6
+    T c1k[3], c3k[3], h6k[3];  // the same times kappa of each field
     C ph[2][3];         // exp(i dk z) at the stage positions z, z+h/2, z+h of each half step
     int skip_rows;      // shipped quirk: transform only row y = 0 (tiles with y != 0 skip)
     unsigned nx;        // grid width (for the row test above)
@@ -99,6 +100,17 @@ struct PassVariant {
 };
 
 inline int max_radix(bool fp64, int threads) { return (fp64 && threads == 128) ? 8 : 16; }
+
+// Whether (threads, r1) is one of the compiled variants (OPO_T_VARIANTS / OPO_A_VARIANTS
+// in ssfm_kernels.cu) for the t-pass (tpass = true) or the axis passes.
+inline bool variant_compiled(bool fp64, bool tpass, PassVariant v)
+{
+    if (v.threads != 128 && v.threads != 256) return false;
+    if (v.r1 != 4 && v.r1 != 8 && v.r1 != 16) return false;
+    if (!fp64) return true;
+    if (v.threads == 128 || tpass) return v.r1 <= 8;
+    return true;
+}
 
 // Launchers (ssfm_kernels.cu).  smem in bytes; grid = number of CTAs.  They return
 // cudaErrorInvalidValue for a variant that is not compiled.

@@ -189,6 +189,42 @@ __device__ __forceinline__ void cwe_rhs_phase(const T *kap, const C &ph, C p, C 
     di = cmul(di, ph);
 }
 
+// The products u_p = s i, u_s = p i*, u_i = p s* give k = i kappa u, so every use of k
+// (the next stage's A + c k and the final sum) folds kappa and the step weights into
+// precomputed constants: A + c k = (A.x - c kappa u.y, A.y + c kappa u.x), and
+// A += (h/6) kappa i (u1 + 2 u2 + 2 u3 + u4).
+template <typename C, typename T>
+__device__ __forceinline__ C add_iku(C a, T ck, C u)
+{
+    return C{a.x - ck * u.y, a.y + ck * u.x};
+}
+
+template <typename C>
+__device__ __forceinline__ void rk4_half_fast(const TPassArgs<C> &a, C &p, C &s, C &i)
+{
+    using T = typename TPassArgs<C>::T;
+    C up = cmul(s, i), us = cmulc(p, i), ui = cmulc(p, s);  // stage 1
+    C Up = up, Us = us, Ui = ui;
+    C p2 = add_iku(p, a.c1k[0], up), s2 = add_iku(s, a.c1k[1], us), i2 = add_iku(i, a.c1k[2], ui);
+    up = cmul(s2, i2); us = cmulc(p2, i2); ui = cmulc(p2, s2);  // stage 2
+    Up = C{Up.x + T(2) * up.x, Up.y + T(2) * up.y};
+    Us = C{Us.x + T(2) * us.x, Us.y + T(2) * us.y};
+    Ui = C{Ui.x + T(2) * ui.x, Ui.y + T(2) * ui.y};
+    p2 = add_iku(p, a.c1k[0], up); s2 = add_iku(s, a.c1k[1], us); i2 = add_iku(i, a.c1k[2], ui);
+    up = cmul(s2, i2); us = cmulc(p2, i2); ui = cmulc(p2, s2);  // stage 3
+    Up = C{Up.x + T(2) * up.x, Up.y + T(2) * up.y};
+    Us = C{Us.x + T(2) * us.x, Us.y + T(2) * us.y};
+    Ui = C{Ui.x + T(2) * ui.x, Ui.y + T(2) * ui.y};
+    p2 = add_iku(p, a.c3k[0], up); s2 = add_iku(s, a.c3k[1], us); i2 = add_iku(i, a.c3k[2], ui);
+    up = cmul(s2, i2); us = cmulc(p2, i2); ui = cmulc(p2, s2);  // stage 4
+    Up = C{Up.x + up.x, Up.y + up.y};
+    Us = C{Us.x + us.x, Us.y + us.y};
+    Ui = C{Ui.x + ui.x, Ui.y + ui.y};
+    p = add_iku(p, a.h6k[0], Up);
+    s = add_iku(s, a.h6k[1], Us);
+    i = add_iku(i, a.h6k[2], Ui);
+}
+
 template <typename C>
 __device__ __forceinline__ void rk4_half(const TPassArgs<C> &a, int h, C &p, C &s, C &i)
 {
@@ -196,13 +232,8 @@ __device__ __forceinline__ void rk4_half(const TPassArgs<C> &a, int h, C &p, C &
     C k1p, k1s, k1i, k2p, k2s, k2i, k3p, k3s, k3i, k4p, k4s, k4i;
     const T c1 = a.c1, c3 = a.c3;
     if (!a.use_phase) {
-        cwe_rhs(a.kappa, p, s, i, k1p, k1s, k1i);
-        cwe_rhs(a.kappa, C{p.x + c1 * k1p.x, p.y + c1 * k1p.y}, C{s.x + c1 * k1s.x, s.y + c1 * k1s.y},
-                C{i.x + c1 * k1i.x, i.y + c1 * k1i.y}, k2p, k2s, k2i);
-        cwe_rhs(a.kappa, C{p.x + c1 * k2p.x, p.y + c1 * k2p.y}, C{s.x + c1 * k2s.x, s.y + c1 * k2s.y},
-                C{i.x + c1 * k2i.x, i.y + c1 * k2i.y}, k3p, k3s, k3i);
-        cwe_rhs(a.kappa, C{p.x + c3 * k3p.x, p.y + c3 * k3p.y}, C{s.x + c3 * k3s.x, s.y + c3 * k3s.y},
-                C{i.x + c3 * k3i.x, i.y + c3 * k3i.y}, k4p, k4s, k4i);
+        rk4_half_fast(a, p, s, i);
+        return;
     } else {
         const C *ph = a.ph[h];
         cwe_rhs_phase(a.kappa, ph[0], p, s, i, k1p, k1s, k1i);
