@@ -86,8 +86,26 @@ def lib():
         L.opo_field_sums.argtypes = [vp, dp]
         L.opo_synchronize.argtypes = [vp]
         L.opo_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.opo_init_fields.argtypes = [vp, ctypes.POINTER(OpoConfig), ctypes.c_uint64, _d, _i]
+        L.opo_batch_create.argtypes = [_i, _i, ctypes.c_size_t, ctypes.POINTER(_i), ctypes.POINTER(vp)]
+        L.opo_batch_destroy.argtypes = [vp]
+        L.opo_batch_destroy.restype = None
+        L.opo_batch_add.argtypes = [vp, ctypes.POINTER(OpoParams), dp, ctypes.POINTER(_i)]
+        L.opo_batch_remove.argtypes = [vp, _i]
+        L.opo_batch_set_field.argtypes = [vp, _i, _i, vp, _i, _i]
+        L.opo_batch_get_field.argtypes = [vp, _i, _i, vp, _i, _i]
+        L.opo_batch_init_fields.argtypes = [vp, _i, ctypes.POINTER(OpoConfig), ctypes.c_uint64, _d, _i]
+        L.opo_batch_run_round_trips.argtypes = [vp, _i]
+        L.opo_batch_sums.argtypes = [vp, dp]
+        L.opo_batch_info.argtypes = [vp, _i, ctypes.POINTER(ctypes.c_longlong)]
+        L.opo_batch_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.opo_batch_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.opo_batch_synchronize.argtypes = [vp]
+        L.opo_batch_last_error.argtypes = [vp]
+        L.opo_batch_last_error.restype = ctypes.c_char_p
         L.opo_autotune.argtypes = [vp]
         L.opo_get_tuning.argtypes = [vp, ctypes.POINTER(_i)]
+        L.opo_set_tuning.argtypes = [vp, ctypes.POINTER(_i)]
         L.opo_field_sums_noalloc.argtypes = [vp, vp, vp, ctypes.c_size_t, _i, vp, dp]
         L.opo_set_pass_timing.argtypes = [vp, _i]
         L.opo_pass_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong)]
@@ -221,12 +239,22 @@ class Simulation:
         self._check(lib().opo_autotune(self._h))
         return self.tuning
 
+    def set_tuning(self, tuning):
+        flat = []
+        for k in ("t", "x", "y"):
+            flat += [tuning[k]["threads"], tuning[k]["tile"], tuning[k]["r1"]]
+        self._check(lib().opo_set_tuning(self._h, (_i * 9)(*flat)))
+
     @property
     def tuning(self):
         out = (_i * 9)()
         self._check(lib().opo_get_tuning(self._h, out))
         return {k: dict(threads=out[3 * i], tile=out[3 * i + 1], r1=out[3 * i + 2])
                 for i, k in enumerate(("t", "x", "y"))}
+
+    def init_fields(self, cfg, seed, sigma, idler_copy=False):
+        """Api = Ap = pump, As = seeded noise, Ai = 0 (or As), computed on the device."""
+        self._check(lib().opo_init_fields(self._h, ctypes.byref(cfg), seed, sigma, 1 if idler_copy else 0))
 
     def set_pass_timing(self, enable):
         self._check(lib().opo_set_pass_timing(self._h, 1 if enable else 0))
@@ -252,6 +280,99 @@ class Simulation:
     def close(self):
         if self._h:
             lib().opo_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many instances advanced together by one persistent launch per pass
+    (opo_batch_* of the C-ABI).  Instances are admitted into slots while they fit the
+    HBM budget; all take the same number of z-steps."""
+
+    def __init__(self, precision, capacity, hbm_budget, tuning=None):
+        self._h = ctypes.c_void_p()
+        self.capacity = capacity
+        self.precision = precision
+        t = None
+        if tuning is not None:
+            flat = []
+            for k in ("t", "x", "y"):
+                flat += [tuning[k]["threads"], tuning[k]["tile"], tuning[k]["r1"]]
+            t = (_i * 9)(*flat)
+        rc = lib().opo_batch_create(precision, capacity, int(hbm_budget), t, ctypes.byref(self._h))
+        if rc:
+            raise OpoError(rc, lib().opo_batch_last_error(None).decode())
+        self.shapes = {}
+
+    def _check(self, rc):
+        if rc:
+            raise OpoError(rc, lib().opo_batch_last_error(self._h).decode())
+
+    def add(self, cfg):
+        """Admit the instance of config `cfg`; returns its slot (OpoError code 6 if full)."""
+        params, _ = derive(cfg)
+        _, w = time_freq(cfg.nt, params.t_window)
+        slot = ctypes.c_int(-1)
+        self._check(lib().opo_batch_add(self._h, ctypes.byref(params), _dptr(np.ascontiguousarray(w)),
+                                        ctypes.byref(slot)))
+        self.shapes[slot.value] = (cfg.nt, cfg.ny, cfg.nx)
+        return slot.value
+
+    def remove(self, slot):
+        self._check(lib().opo_batch_remove(self._h, slot))
+        self.shapes.pop(slot, None)
+
+    def init_fields(self, slot, cfg, seed, sigma, idler_copy=False):
+        self._check(lib().opo_batch_init_fields(self._h, slot, ctypes.byref(cfg), seed, sigma,
+                                                1 if idler_copy else 0))
+
+    def set_field(self, slot, which, arr):
+        a = np.ascontiguousarray(arr, dtype=np.complex128).reshape(-1)
+        self._check(lib().opo_batch_set_field(self._h, slot, which, a.ctypes.data_as(ctypes.c_void_p),
+                                              MEM_HOST, FP64))
+
+    def get_field(self, slot, which):
+        shape = self.shapes[slot]
+        a = np.zeros(int(np.prod(shape)), dtype=np.complex128)
+        self._check(lib().opo_batch_get_field(self._h, slot, which, a.ctypes.data_as(ctypes.c_void_p),
+                                              MEM_HOST, FP64))
+        return a.reshape(shape)
+
+    def run_round_trips(self, n):
+        self._check(lib().opo_batch_run_round_trips(self._h, n))
+
+    def sums(self):
+        s = np.zeros(3 * self.capacity)
+        self._check(lib().opo_batch_sums(self._h, _dptr(s)))
+        return s.reshape(self.capacity, 3)
+
+    def info(self, slot):
+        out = (ctypes.c_longlong * 4)()
+        self._check(lib().opo_batch_info(self._h, slot, out))
+        return dict(round_trips=out[0], total_rt=out[1], voxels=out[2], bytes=out[3])
+
+    def stats(self):
+        out = (ctypes.c_longlong * 4)()
+        self._check(lib().opo_batch_stats(self._h, out))
+        return dict(instances=out[0], used=out[1], budget=out[2], launches=out[3])
+
+    @property
+    def stream(self):
+        st = ctypes.c_void_p()
+        self._check(lib().opo_batch_get_stream(self._h, ctypes.byref(st)))
+        return st.value or 0
+
+    def synchronize(self):
+        self._check(lib().opo_batch_synchronize(self._h))
+
+    def close(self):
+        if self._h:
+            lib().opo_batch_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

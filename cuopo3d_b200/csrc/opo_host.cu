@@ -4,6 +4,7 @@
 
 #include "../../include/cuopo3d.h"
 #include "opo_internal.h"
+#include "solver_internal.h"
 
 #include <cmath>
 #include <complex>
@@ -232,6 +233,7 @@ struct OpoSolver {
     OpoParams p{};
     std::string err;
     cudaStream_t stream = nullptr;
+    bool own_stream = true;
     int dev = 0;
     size_t V = 0;
     size_t esz = 0;  // bytes per complex element
@@ -481,15 +483,21 @@ template <typename C> typename opo::TabOf<C>::type *const *tabs(OpoSolver *s, in
     return reinterpret_cast<typename opo::TabOf<C>::type *const *>(s->pass[kind].tab[which]);
 }
 
-// One t-pass.  n_rk4 half steps (z of each given), then, for the fields in tmask,
-// transform -> table -> inverse.
+}  // namespace
+
+namespace opo {
+
+// Arguments of one t-pass of solver s: n_rk4 half steps (z of each given), then, for the
+// fields in tmask, transform -> table `which_tab` (0 crystal, 1 round-trip boundary) ->
+// inverse.
 template <typename C>
-int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, int which_tab, unsigned tmask)
+TPassArgs<C> make_tpass_args(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, int which_tab,
+                             unsigned tmask)
 {
     const OpoParams &p = s->p;
     const PassCfg &pc = s->pass[kT];
-    opo::TPassArgs<C> a{};
-    using T = typename opo::TPassArgs<C>::T;
+    TPassArgs<C> a{};
+    using T = typename TPassArgs<C>::T;
     for (int f = 0; f < 3; f++) a.f[f] = fld<C>(s, f + 1);
     a.psrc = reset_pump ? fld<C>(s, 0) : fld<C>(s, 1);
     a.g = pc.geo;
@@ -517,6 +525,31 @@ int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, int wh
     }
     a.skip_rows = (p.flags & OPO_ASIS_Q2) ? 1 : 0;
     a.nx = (unsigned)p.nx;
+    return a;
+}
+
+template <typename C> AxisArgs<C> make_axis_args(OpoSolver *s, int kind, int which_tab, unsigned mask)
+{
+    const PassCfg &pc = s->pass[kind];
+    AxisArgs<C> a{};
+    for (int f = 0; f < 3; f++) a.f[f] = fld<C>(s, f + 1);
+    a.g = pc.geo;
+    a.plan = pc.plan;
+    a.tw = static_cast<const C *>(pc.tw);
+    for (int f = 0; f < 3; f++) a.tab[f] = tabs<C>(s, kind, which_tab)[f];
+    a.tmask = mask;
+    return a;
+}
+
+}  // namespace opo
+
+namespace {
+
+template <typename C>
+int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, int which_tab, unsigned tmask)
+{
+    const PassCfg &pc = s->pass[kT];
+    const opo::TPassArgs<C> a = opo::make_tpass_args<C>(s, reset_pump, n_rk4, zh, which_tab, tmask);
     PassTimer timer(s, 0);
     OPO_CU(s, opo::launch_tpass<C>(a, pc.v, a.g.ntiles, pc.smem, s->stream), "t-pass launch");
     s->launches++;
@@ -526,13 +559,7 @@ int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, int wh
 template <typename C> int enqueue_axis(OpoSolver *s, int kind, int which_tab, unsigned mask)
 {
     const PassCfg &pc = s->pass[kind];
-    opo::AxisArgs<C> a{};
-    for (int f = 0; f < 3; f++) a.f[f] = fld<C>(s, f + 1);
-    a.g = pc.geo;
-    a.plan = pc.plan;
-    a.tw = static_cast<const C *>(pc.tw);
-    for (int f = 0; f < 3; f++) a.tab[f] = tabs<C>(s, kind, which_tab)[f];
-    a.tmask = mask;
+    const opo::AxisArgs<C> a = opo::make_axis_args<C>(s, kind, which_tab, mask);
     PassTimer timer(s, kind);
     OPO_CU(s, opo::launch_axis<C>(a, pc.v, kind == kX, a.g.ntiles, pc.smem, s->stream), "axis-pass launch");
     s->launches++;
@@ -919,7 +946,8 @@ int opo_noise(uint64_t seed, double sigma, size_t n, double *out)
     return OPO_OK;
 }
 
-int opo_create(const OpoParams *p, const double *w, OpoSolver **out)
+static int create_impl(const OpoParams *p, const double *w, const opo::PassVariant *vv, const size_t *tt,
+                       cudaStream_t ext_stream, OpoSolver **out)
 {
     if (!out) return OPO_ERR_INVALID;
     *out = nullptr;
@@ -937,7 +965,10 @@ int opo_create(const OpoParams *p, const double *w, OpoSolver **out)
     cudaError_t e;
     do {
         if ((e = cudaGetDevice(&s->dev)) != cudaSuccess) { rc = cuda_fail(s, e, "cudaGetDevice"); break; }
-        if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        if (ext_stream) {
+            s->stream = ext_stream;
+            s->own_stream = false;
+        } else if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess) {
             rc = cuda_fail(s, e, "stream");
             break;
         }
@@ -956,6 +987,10 @@ int opo_create(const OpoParams *p, const double *w, OpoSolver **out)
             opo::PassVariant v;
             size_t te;
             default_variant(p->precision == OPO_FP64, k, v, te);
+            if (vv && tt) {
+                v = vv[k];
+                te = tt[k];
+            }
             rc = p->precision == OPO_FP64 ? configure_pass<double2>(s, k, v, te) : configure_pass<float2>(s, k, v, te);
         }
         if (rc) break;
@@ -977,6 +1012,11 @@ int opo_create(const OpoParams *p, const double *w, OpoSolver **out)
     return OPO_OK;
 }
 
+int opo_create(const OpoParams *p, const double *w, OpoSolver **out)
+{
+    return create_impl(p, w, nullptr, nullptr, nullptr, out);
+}
+
 void opo_destroy(OpoSolver *s)
 {
     if (!s) return;
@@ -993,7 +1033,7 @@ void opo_destroy(OpoSolver *s)
     if (s->partials) cudaFree(s->partials);
     if (s->staging) cudaFree(s->staging);
     for (auto &pc : s->pass) free_pass(pc);
-    if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
     delete s;
 }
 
@@ -1101,10 +1141,30 @@ int opo_pass_times(OpoSolver *s, double ms[4], long long counts[4])
     return OPO_OK;
 }
 
+int opo_init_fields(OpoSolver *s, const OpoConfig *cfg, uint64_t seed, double sigma, int idler_copy)
+{
+    if (!s || !cfg) return s ? fail(s, OPO_ERR_INVALID, "null configuration") : OPO_ERR_INVALID;
+    int rc = opo::init_fields_device(s, cfg, seed, sigma, idler_copy, s->stream);
+    if (!rc) s->launches++;
+    return rc;
+}
+
 int opo_autotune(OpoSolver *s)
 {
     if (!s) return OPO_ERR_INVALID;
     return s->p.precision == OPO_FP64 ? autotune<double2>(s) : autotune<float2>(s);
+}
+
+int opo_set_tuning(OpoSolver *s, const int tuning[9])
+{
+    if (!s || !tuning) return OPO_ERR_INVALID;
+    for (int k = 0; k < 3; k++) {
+        const opo::PassVariant v{tuning[3 * k], tuning[3 * k + 2]};
+        const size_t te = (size_t)tuning[3 * k + 1];
+        int rc = s->p.precision == OPO_FP64 ? configure_pass<double2>(s, k, v, te) : configure_pass<float2>(s, k, v, te);
+        if (rc) return rc;
+    }
+    return OPO_OK;
 }
 
 int opo_get_tuning(const OpoSolver *s, int out[9])
@@ -1130,3 +1190,69 @@ long long opo_kernel_launches(const OpoSolver *s) { return s ? s->launches : -1;
 const char *opo_last_error(const OpoSolver *s) { return s ? s->err.c_str() : g_static_err; }
 
 }  // extern "C"
+
+namespace opo {
+
+int solver_create_configured(const OpoParams *p, const double *w, const PassVariant v[3], const size_t te[3],
+                             cudaStream_t stream, OpoSolver **out)
+{
+    return create_impl(p, w, v, te, stream, out);
+}
+
+PassVariant solver_pass_variant(const OpoSolver *s, int kind) { return s->pass[kind].v; }
+
+void solver_pass_info(const OpoSolver *s, int kind, int *ntiles, size_t *smem)
+{
+    *ntiles = s->pass[kind].geo.ntiles;
+    *smem = s->pass[kind].smem;
+}
+
+const OpoParams &solver_params(const OpoSolver *s) { return s->p; }
+
+size_t solver_device_bytes(const OpoSolver *s)
+{
+    size_t b = 4 * s->esz * s->V + 3 * sizeof(double) * (s->sum_blocks + 1);
+    return b;
+}
+
+void *solver_field(OpoSolver *s, int which) { return s->field[which]; }
+
+cudaStream_t solver_stream(const OpoSolver *s) { return s->stream; }
+
+bool solver_gdd_or_mirror(const OpoSolver *s) { return s->gdd_or_mirror; }
+
+void solver_tpass_z(const OpoParams &p, int tp, double zh[2], int *n_rk4)
+{
+    const bool phys = (p.flags & OPO_PHYSICS) != 0;
+    if (tp == 0) {
+        zh[0] = step_z(p, 0);
+        zh[1] = 0;
+        *n_rk4 = 1;
+    } else if (tp < p.n_steps) {
+        zh[0] = phys ? step_z(p, tp - 1) + 0.5 * p.dz : step_z(p, tp - 1);
+        zh[1] = step_z(p, tp);
+        *n_rk4 = 2;
+    } else {
+        zh[0] = last_half_z(p);
+        zh[1] = 0;
+        *n_rk4 = 1;
+    }
+}
+
+int solver_fail(OpoSolver *s, int code, const char *msg) { return fail(s, code, msg); }
+
+void solver_release_staging(OpoSolver *s)
+{
+    if (s->staging) {
+        cudaStreamSynchronize(s->stream);
+        cudaFree(s->staging);
+        s->staging = nullptr;
+    }
+}
+
+template TPassArgs<float2> make_tpass_args<float2>(OpoSolver *, bool, int, const double *, int, unsigned);
+template TPassArgs<double2> make_tpass_args<double2>(OpoSolver *, bool, int, const double *, int, unsigned);
+template AxisArgs<float2> make_axis_args<float2>(OpoSolver *, int, int, unsigned);
+template AxisArgs<double2> make_axis_args<double2>(OpoSolver *, int, int, unsigned);
+
+}  // namespace opo

@@ -79,6 +79,7 @@ template <typename C> struct TPassArgs {
     T c1, c3, h6;       // RK4 stage offsets (k1, k2 -> c1; k3 -> c3) and final weight h/6
     T c1k[3], c3k[3], h6k[3];  // the same times kappa of each field
     C ph[2][3];         // exp(i dk z) at the stage positions z, z+h/2, z+h of each half step
+    const C *ph_steps;  // batched passes: the ph values of every t-pass of a round trip, [tp][2][3]
     int skip_rows;      // shipped quirk: transform only row y = 0 (tiles with y != 0 skip)
     unsigned nx;        // grid width (for the row test above)
 };

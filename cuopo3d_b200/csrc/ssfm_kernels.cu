@@ -1,354 +1,21 @@
-// Pass kernels of the split-step solver for sm_100a.
-//
-// Every z-step of the reference (Solver3D.cuh:946-960: RK4(dz/2), dispersion,
-// diffraction, RK4(dz/2)) is executed as three passes over the resident fields, each
-// reading and writing the three complex fields once:
-//   t-pass    coupled-wave RK4 half steps (all stages in registers) fused with the
-//             t-axis operator: transform, times the dispersion phase, inverse transform
-//   x-pass,   the separable diffraction operator exp(-i dz 2 pi^2 (fx^2 + fy^2) / k)
-//   y-pass    = (x factor) (y factor), one axis per pass.
-// A CTA owns a tile of whole lines of one axis for all three fields: lines are staged
-// in shared memory with the line index fastest (so every stage is bank-conflict free),
-// the first transform stage is fused with the coalesced global load (and, in the
-// t-pass, with the RK4 update) and the last inverse stage with the global store.  The
-// middle stages exchange through shared memory; the last forward stage, the phase
-// multiply and the first inverse stage are one register-resident step.
-//
-// Index arithmetic is 32-bit (a field holds fewer than 2^32 values) and every division
-// by a run-time invariant uses a precomputed multiply-high (FastDiv).
+// Single-instance pass kernels of the split-step solver for sm_100a (the tile bodies
+// are in pass_body.cuh), the FP64 tallies, precision conversions and the launchers.
 
-#include "fft_radix.cuh"
-#include "opo_internal.h"
+#include <type_traits>
+
+#include "pass_body.cuh"
 
 namespace opo {
 
-template <int S, typename C> __device__ __forceinline__ C twmul(C x, C w)
-{
-    // w holds exp(-2 pi i e / L); a stage of sign S multiplies by exp(S 2 pi i e / L)
-    return S < 0 ? cmul(x, w) : cmulc(x, w);
-}
-
-__device__ __forceinline__ double2 tab_mul(double2 x, double2 t) { return cmul(x, t); }
-__device__ __forceinline__ float2 tab_mul(float2 x, float4 t)
-{
-    const float2 a = cmul(x, make_float2(t.x, t.y)), b = cmul(x, make_float2(t.z, t.w));
-    return make_float2(a.x + b.x, a.y + b.y);
-}
-
-__device__ __forceinline__ unsigned tile_base(const TileGeom &g, unsigned tile)
-{
-    const unsigned hi = fdiv(g.tdiv, tile);
-    return (tile - hi * g.tdiv.d) * g.tmulA + hi * g.tmulB;
-}
-
-// Index of the f-th field (in p, s, i order) selected by mask.
-__device__ __forceinline__ int field_id(unsigned mask, int f)
-{
-    for (int k = 0; k < 3; k++)
-        if (mask & (1u << k)) {
-            if (f == 0) return k;
-            f--;
-        }
-    return 0;
-}
-
-// ---------------------------------------------------------------------------------
-// Shared-memory stages.  Per field, work item w -> (line l fastest, butterfly b).
-
-template <typename C, int R, int S, bool DIT, int THREADS>
-__device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv &fq, const C *tw, int nf)
-{
-    const unsigned q = fq.d, nl = (unsigned)g.nlines, LS = (unsigned)g.LS;
-    const unsigned items = (unsigned)(n / R) * nl;
-    for (int f = 0; f < nf; f++) {
-        C *sf = sm + (size_t)f * n * LS;
-        for (unsigned w = threadIdx.x; w < items; w += THREADS) {
-            const unsigned b = fdiv(g.nl, w), l = w - b * nl;
-            const unsigned gq = fdiv(fq, b), j = b - gq * q;
-            C *s = sf + (gq * L + j) * LS + l;
-            C x[R];
-#pragma unroll
-            for (int m = 0; m < R; m++) x[m] = s[m * q * LS];
-            if (DIT && q > 1) {
-#pragma unroll
-                for (int m = 1; m < R; m++) x[m] = twmul<S>(x[m], __ldg(tw + (m - 1) * q + j));
-            }
-            dft<R, S>(x);
-            if (!DIT && q > 1) {
-#pragma unroll
-                for (int k = 1; k < R; k++) x[k] = twmul<S>(x[k], __ldg(tw + (k - 1) * q + j));
-            }
-#pragma unroll
-            for (int k = 0; k < R; k++) s[k * q * LS] = x[k];
-        }
-    }
-}
-
-// Last forward stage (q = 1), phase multiply, first inverse stage, in registers.
-template <typename C, int R, int SF, int THREADS>
-__device__ void fused_middle(C *sm, const TileGeom &g, int n, const typename TabOf<C>::type *const *tab,
-                             unsigned tmask, int nf)
-{
-    const unsigned nl = (unsigned)g.nlines, LS = (unsigned)g.LS;
-    const unsigned items = (unsigned)(n / R) * nl;
-    for (int f = 0; f < nf; f++) {
-        C *sf = sm + (size_t)f * n * LS;
-        const typename TabOf<C>::type *tf = tab[field_id(tmask, f)];
-        for (unsigned w = threadIdx.x; w < items; w += THREADS) {
-            const unsigned g0 = fdiv(g.nl, w), l = w - g0 * nl;
-            C *s = sf + g0 * R * LS + l;
-            const typename TabOf<C>::type *tb = tf + g0 * R;
-            C x[R];
-#pragma unroll
-            for (int m = 0; m < R; m++) x[m] = s[m * LS];
-            dft<R, SF>(x);
-#pragma unroll
-            for (int k = 0; k < R; k++) x[k] = tab_mul(x[k], __ldg(tb + k));
-            dft<R, -SF>(x);
-#pragma unroll
-            for (int k = 0; k < R; k++) s[k * LS] = x[k];
-        }
-    }
-}
-
-template <typename C, int S, bool DIT, int THREADS, int RMAX>
-__device__ void smem_stage_dispatch(int R, C *sm, const TileGeom &g, int n, int L, const FastDiv &fq,
-                                    const C *tw, int nf)
-{
-    switch (R) {
-    case 2: smem_stage<C, 2, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf); break;
-    case 3: smem_stage<C, 3, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf); break;
-    case 4: smem_stage<C, 4, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf); break;
-    case 8: smem_stage<C, 8, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf); break;
-    case 16:
-        if constexpr (RMAX >= 16) smem_stage<C, 16, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf);
-        break;
-    default: break;
-    }
-}
-
-template <typename C, int SF, int THREADS, int RMAX>
-__device__ void fused_dispatch(int R, C *sm, const TileGeom &g, int n, const typename TabOf<C>::type *const *tab,
-                               unsigned tmask, int nf)
-{
-    switch (R) {
-    case 2: fused_middle<C, 2, SF, THREADS>(sm, g, n, tab, tmask, nf); break;
-    case 3: fused_middle<C, 3, SF, THREADS>(sm, g, n, tab, tmask, nf); break;
-    case 4: fused_middle<C, 4, SF, THREADS>(sm, g, n, tab, tmask, nf); break;
-    case 8: fused_middle<C, 8, SF, THREADS>(sm, g, n, tab, tmask, nf); break;
-    case 16:
-        if constexpr (RMAX >= 16) fused_middle<C, 16, SF, THREADS>(sm, g, n, tab, tmask, nf);
-        break;
-    default: break;
-    }
-}
-
-// Stages 1 .. ns-1 forward, fused middle, inverse back to stage 1 (stage 0 is fused
-// with the global load / store by the caller).
-template <typename C, int SF, int THREADS, int RMAX>
-__device__ void middle_stages(C *sm, const TileGeom &g, const AxisPlan &p, const C *tw,
-                              const typename TabOf<C>::type *const *tab, unsigned tmask, int nf)
-{
-    for (int s = 1; s < p.ns - 1; s++) {
-        smem_stage_dispatch<C, SF, false, THREADS, RMAX>(p.radix[s], sm, g, p.n, p.len[s], p.q[s],
-                                                         tw + p.twoff[s], nf);
-        __syncthreads();
-    }
-    fused_dispatch<C, SF, THREADS, RMAX>(p.radix[p.ns - 1], sm, g, p.n, tab, tmask, nf);
-    __syncthreads();
-    for (int s = p.ns - 2; s >= 1; s--) {
-        smem_stage_dispatch<C, -SF, true, THREADS, RMAX>(p.radix[s], sm, g, p.n, p.len[s], p.q[s],
-                                                         tw + p.twoff[s], nf);
-        __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------------
-// Coupled-wave equations, reference Solver3D.cuh:365-425 and :872-943.
-//   dAp = i kp As Ai e^{-i dk z}, dAs = i ks Ap Ai* e^{i dk z}, dAi = i ki Ap As* e^{i dk z}
-// One half step of size h = dz/2: k1 = f(A), k2 = f(A + c1 k1), k3 = f(A + c1 k2),
-// k4 = f(A + c3 k3), A += (k1 + 2 k2 + 2 k3 + k4) h / 6.  The shipped stage offsets are
-// c1 = 0.5, c3 = 1 (no step size); corrected physics uses c1 = h/2, c3 = h.
-
-template <typename C, typename T>
-__device__ __forceinline__ void cwe_rhs(const T *kap, C p, C s, C i, C &dp, C &ds, C &di)
-{
-    C si = cmul(s, i), pic = cmulc(p, i), psc = cmulc(p, s);
-    dp = C{-kap[0] * si.y, kap[0] * si.x};
-    ds = C{-kap[1] * pic.y, kap[1] * pic.x};
-    di = C{-kap[2] * psc.y, kap[2] * psc.x};
-}
-
-template <typename C, typename T>
-__device__ __forceinline__ void cwe_rhs_phase(const T *kap, const C &ph, C p, C s, C i, C &dp, C &ds,
-                                              C &di)
-{
-    cwe_rhs(kap, p, s, i, dp, ds, di);
-    dp = cmulc(dp, ph);
-    ds = cmul(ds, ph);
-    di = cmul(di, ph);
-}
-
-// The products u_p = s i, u_s = p i*, u_i = p s* give k = i kappa u, so every use of k
-// (the next stage's A + c k and the final sum) folds kappa and the step weights into
-// precomputed constants: A + c k = (A.x - c kappa u.y, A.y + c kappa u.x), and
-// A += (h/6) kappa i (u1 + 2 u2 + 2 u3 + u4).
-template <typename C, typename T>
-__device__ __forceinline__ C add_iku(C a, T ck, C u)
-{
-    return C{a.x - ck * u.y, a.y + ck * u.x};
-}
-
-template <typename C>
-__device__ __forceinline__ void rk4_half_fast(const TPassArgs<C> &a, C &p, C &s, C &i)
-{
-    using T = typename TPassArgs<C>::T;
-    C up = cmul(s, i), us = cmulc(p, i), ui = cmulc(p, s);  // stage 1
-    C Up = up, Us = us, Ui = ui;
-    C p2 = add_iku(p, a.c1k[0], up), s2 = add_iku(s, a.c1k[1], us), i2 = add_iku(i, a.c1k[2], ui);
-    up = cmul(s2, i2); us = cmulc(p2, i2); ui = cmulc(p2, s2);  // stage 2
-    Up = C{Up.x + T(2) * up.x, Up.y + T(2) * up.y};
-    Us = C{Us.x + T(2) * us.x, Us.y + T(2) * us.y};
-    Ui = C{Ui.x + T(2) * ui.x, Ui.y + T(2) * ui.y};
-    p2 = add_iku(p, a.c1k[0], up); s2 = add_iku(s, a.c1k[1], us); i2 = add_iku(i, a.c1k[2], ui);
-    up = cmul(s2, i2); us = cmulc(p2, i2); ui = cmulc(p2, s2);  // stage 3
-    Up = C{Up.x + T(2) * up.x, Up.y + T(2) * up.y};
-    Us = C{Us.x + T(2) * us.x, Us.y + T(2) * us.y};
-    Ui = C{Ui.x + T(2) * ui.x, Ui.y + T(2) * ui.y};
-    p2 = add_iku(p, a.c3k[0], up); s2 = add_iku(s, a.c3k[1], us); i2 = add_iku(i, a.c3k[2], ui);
-    up = cmul(s2, i2); us = cmulc(p2, i2); ui = cmulc(p2, s2);  // stage 4
-    Up = C{Up.x + up.x, Up.y + up.y};
-    Us = C{Us.x + us.x, Us.y + us.y};
-    Ui = C{Ui.x + ui.x, Ui.y + ui.y};
-    p = add_iku(p, a.h6k[0], Up);
-    s = add_iku(s, a.h6k[1], Us);
-    i = add_iku(i, a.h6k[2], Ui);
-}
-
-template <typename C>
-__device__ __forceinline__ void rk4_half(const TPassArgs<C> &a, int h, C &p, C &s, C &i)
-{
-    using T = typename TPassArgs<C>::T;
-    C k1p, k1s, k1i, k2p, k2s, k2i, k3p, k3s, k3i, k4p, k4s, k4i;
-    const T c1 = a.c1, c3 = a.c3;
-    if (!a.use_phase) {
-        rk4_half_fast(a, p, s, i);
-        return;
-    } else {
-        const C *ph = a.ph[h];
-        cwe_rhs_phase(a.kappa, ph[0], p, s, i, k1p, k1s, k1i);
-        cwe_rhs_phase(a.kappa, ph[1], C{p.x + c1 * k1p.x, p.y + c1 * k1p.y},
-                      C{s.x + c1 * k1s.x, s.y + c1 * k1s.y}, C{i.x + c1 * k1i.x, i.y + c1 * k1i.y},
-                      k2p, k2s, k2i);
-        cwe_rhs_phase(a.kappa, ph[1], C{p.x + c1 * k2p.x, p.y + c1 * k2p.y},
-                      C{s.x + c1 * k2s.x, s.y + c1 * k2s.y}, C{i.x + c1 * k2i.x, i.y + c1 * k2i.y},
-                      k3p, k3s, k3i);
-        cwe_rhs_phase(a.kappa, ph[2], C{p.x + c3 * k3p.x, p.y + c3 * k3p.y},
-                      C{s.x + c3 * k3s.x, s.y + c3 * k3s.y}, C{i.x + c3 * k3i.x, i.y + c3 * k3i.y},
-                      k4p, k4s, k4i);
-    }
-    const T w = a.h6;
-    p.x += (k1p.x + T(2) * k2p.x + T(2) * k3p.x + k4p.x) * w;
-    p.y += (k1p.y + T(2) * k2p.y + T(2) * k3p.y + k4p.y) * w;
-    s.x += (k1s.x + T(2) * k2s.x + T(2) * k3s.x + k4s.x) * w;
-    s.y += (k1s.y + T(2) * k2s.y + T(2) * k3s.y + k4s.y) * w;
-    i.x += (k1i.x + T(2) * k2i.x + T(2) * k3i.x + k4i.x) * w;
-    i.y += (k1i.y + T(2) * k2i.y + T(2) * k3i.y + k4i.y) * w;
-}
-
-// ---------------------------------------------------------------------------------
-// t-pass: tile = P consecutive pixels (x) of one row y, all t, all three fields.
-// Stage 0 (radix R1, stride q = nt/R1): each thread loads R1 time samples of one pixel
-// for p, s, i, applies n_rk4 half steps to each voxel, then the first forward stage of
-// every transformed field into shared memory (untransformed fields go straight back).
+// Single-instance kernels: the grid walks the tiles of one solver.
 
 template <typename C, int R1, int THREADS, int RMAX>
 __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 4 : 1) tpass_kernel(TPassArgs<C> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *sm = reinterpret_cast<C *>(smem_raw);
-    const AxisPlan &p = a.plan;
-    const TileGeom &g = a.g;
-    const unsigned n = p.n, q = n / R1, P = g.nlines, LS = g.LS;
-    const int nf = __popc(a.tmask);
-
-    for (unsigned tile = blockIdx.x; tile < (unsigned)g.ntiles; tile += gridDim.x) {
-        const unsigned base = tile_base(g, tile);
-        bool xform = nf > 0;
-        if (a.skip_rows && base >= a.nx) xform = false;  // row y = base / nx != 0
-        for (unsigned w = threadIdx.x; w < q * P; w += THREADS) {
-            const unsigned b = fdiv(g.nl, w), l = w - b * P;
-            const unsigned gb = base + l * g.gs_l + b * g.gs_j;
-            const unsigned gstep = q * g.gs_j;
-            C x[3][R1];
-#pragma unroll
-            for (int m = 0; m < R1; m++) {
-                const unsigned gi = gb + m * gstep;
-                x[0][m] = a.psrc[gi];
-                x[1][m] = a.f[1][gi];
-                x[2][m] = a.f[2][gi];
-            }
-            for (int h = 0; h < a.n_rk4; h++) {
-#pragma unroll
-                for (int m = 0; m < R1; m++) rk4_half(a, h, x[0][m], x[1][m], x[2][m]);
-            }
-#pragma unroll
-            for (int f = 0; f < 3; f++) {
-                if (xform && (a.tmask & (1u << f))) {
-                    dft<R1, +1>(x[f]);
-#pragma unroll
-                    for (int k = 1; k < R1; k++) x[f][k] = twmul<+1>(x[f][k], __ldg(a.tw + (k - 1) * q + b));
-                    C *s = sm + (size_t)__popc(a.tmask & ((1u << f) - 1u)) * n * LS + b * LS + l;
-#pragma unroll
-                    for (int k = 0; k < R1; k++) s[k * q * LS] = x[f][k];
-                } else {
-#pragma unroll
-                    for (int m = 0; m < R1; m++) a.f[f][gb + m * gstep] = x[f][m];
-                }
-            }
-        }
-        if (!xform) continue;
-        __syncthreads();
-        middle_stages<C, +1, THREADS, RMAX>(sm, g, p, a.tw, a.tab, a.tmask, nf);
-        // Stage 0 inverse (sign -1) and store.
-        for (int f = 0; f < nf; f++) {
-            C *sf = sm + (size_t)f * n * LS;
-            C *dstf = a.f[field_id(a.tmask, f)];
-            for (unsigned w = threadIdx.x; w < q * P; w += THREADS) {
-                const unsigned b = fdiv(g.nl, w), l = w - b * P;
-                const C *s = sf + b * LS + l;
-                C x[R1];
-#pragma unroll
-                for (int m = 0; m < R1; m++) x[m] = s[m * q * LS];
-#pragma unroll
-                for (int m = 1; m < R1; m++) x[m] = twmul<-1>(x[m], __ldg(a.tw + (m - 1) * q + b));
-                dft<R1, -1>(x);
-                C *dst = dstf + base + l * g.gs_l + b * g.gs_j;
-#pragma unroll
-                for (int k = 0; k < R1; k++) dst[k * q * g.gs_j] = x[k];
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------------
-// Axis pass (x or y diffraction factor): forward transform sign -1 (the reference's
-// CUFFT_FORWARD), phase, inverse sign +1.  BFAST maps consecutive threads to
-// consecutive butterflies of a line (x axis, where lines are rows and the transform
-// index is the contiguous one); otherwise consecutive threads take consecutive lines.
-
-template <bool BFAST>
-__device__ __forceinline__ void axis_item(unsigned w, const FastDiv &fq, const FastDiv &fnl, unsigned &b,
-                                          unsigned &l)
-{
-    if (BFAST) {
-        l = fdiv(fq, w);
-        b = w - l * fq.d;
-    } else {
-        b = fdiv(fnl, w);
-        l = w - b * fnl.d;
-    }
+    for (unsigned tile = blockIdx.x; tile < (unsigned)a.g.ntiles; tile += gridDim.x)
+        tpass_tile<C, R1, THREADS, RMAX>(a, tile, sm);
 }
 
 template <typename C, int R1, bool BFAST, int THREADS, int RMAX>
@@ -356,54 +23,8 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 4 : 1) axis_kernel(A
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *sm = reinterpret_cast<C *>(smem_raw);
-    const AxisPlan &p = a.plan;
-    const TileGeom &g = a.g;
-    const unsigned n = p.n, q = n / R1, NL = g.nlines, LS = g.LS;
-    const int nf = __popc(a.tmask);
-    const unsigned items = q * NL;
-
-    for (unsigned tile = blockIdx.x; tile < (unsigned)g.ntiles; tile += gridDim.x) {
-        const unsigned base = tile_base(g, tile);
-        for (int f = 0; f < nf; f++) {
-            const C *srcf = a.f[field_id(a.tmask, f)] + base;
-            C *sf = sm + (size_t)f * n * LS;
-            for (unsigned w = threadIdx.x; w < items; w += THREADS) {
-                unsigned b, l;
-                axis_item<BFAST>(w, p.q[0], g.nl, b, l);
-                const C *src = srcf + l * g.gs_l + b * g.gs_j;
-                C x[R1];
-#pragma unroll
-                for (int m = 0; m < R1; m++) x[m] = src[m * q * g.gs_j];
-                dft<R1, -1>(x);
-#pragma unroll
-                for (int k = 1; k < R1; k++) x[k] = twmul<-1>(x[k], __ldg(a.tw + (k - 1) * q + b));
-                C *s = sf + b * LS + l;
-#pragma unroll
-                for (int k = 0; k < R1; k++) s[k * q * LS] = x[k];
-            }
-        }
-        __syncthreads();
-        middle_stages<C, -1, THREADS, RMAX>(sm, g, p, a.tw, a.tab, a.tmask, nf);
-        for (int f = 0; f < nf; f++) {
-            C *dstf = a.f[field_id(a.tmask, f)] + base;
-            const C *sf = sm + (size_t)f * n * LS;
-            for (unsigned w = threadIdx.x; w < items; w += THREADS) {
-                unsigned b, l;
-                axis_item<BFAST>(w, p.q[0], g.nl, b, l);
-                const C *s = sf + b * LS + l;
-                C x[R1];
-#pragma unroll
-                for (int m = 0; m < R1; m++) x[m] = s[m * q * LS];
-#pragma unroll
-                for (int m = 1; m < R1; m++) x[m] = twmul<+1>(x[m], __ldg(a.tw + (m - 1) * q + b));
-                dft<R1, +1>(x);
-                C *dst = dstf + l * g.gs_l + b * g.gs_j;
-#pragma unroll
-                for (int k = 0; k < R1; k++) dst[k * q * g.gs_j] = x[k];
-            }
-        }
-        __syncthreads();
-    }
+    for (unsigned tile = blockIdx.x; tile < (unsigned)a.g.ntiles; tile += gridDim.x)
+        axis_tile<C, R1, BFAST, THREADS, RMAX>(a, tile, sm);
 }
 
 // ---------------------------------------------------------------------------------

@@ -155,6 +155,11 @@ void opo_destroy(OpoSolver *s);
 int opo_set_field(OpoSolver *s, int which, const void *src, int where, int elem_precision);
 int opo_get_field(OpoSolver *s, int which, void *dst, int where, int elem_precision);
 
+/* Initialise the fields on the device from the solver's configuration: Api = Ap = the
+ * pump of opo_pump_field (EFields::setPumpField, EFields3D.cuh:244-296), As = the noise of
+ * opo_noise(seed, sigma) (bit-identical), Ai = 0, or As when idler_copy (cuOPO3D.cu:51). */
+int opo_init_fields(OpoSolver *s, const OpoConfig *cfg, uint64_t seed, double sigma, int idler_copy);
+
 /* One pass through the crystal without cavity, Solver::runSinglePass
  * (Solver3D.cuh:1031-1043; SSFM :946-960). */
 int opo_run_single_pass(OpoSolver *s);
@@ -186,6 +191,11 @@ int opo_pass_times(OpoSolver *s, double ms[4], long long counts[4]);
  * reference's compile-time block sizes (DtypesConsts.cuh:48-50). */
 int opo_autotune(OpoSolver *s);
 
+/* Pin the configuration instead of tuning it (same layout as opo_get_tuning).  Fails
+ * with OPO_ERR_INVALID for a variant that is not compiled or a tile that cannot hold
+ * the grid; the phase tables are rebuilt for the new FFT plans. */
+int opo_set_tuning(OpoSolver *s, const int tuning[9]);
+
 /* Chosen configuration: for the t-, x- and y-pass in turn, {CTA threads, tile elements
  * per field, first-stage radix}.  No counterpart in the reference. */
 int opo_get_tuning(const OpoSolver *s, int out[9]);
@@ -216,6 +226,40 @@ int opo_round_trip_index(const OpoSolver *s);
 long long opo_kernel_launches(const OpoSolver *s);
 const char *opo_last_error(const OpoSolver *s);
 const char *opo_version(void);
+
+/* ---- batched form: many instances, one persistent launch per pass ----------------- */
+
+/* A batch advances every admitted instance (uneven grids and parameters, one slot
+ * each) by whole cavity round trips, with one persistent kernel launch per pass for all
+ * of them and each round trip replayed as one CUDA graph.  Instances are admitted while
+ * their device memory fits the HBM budget; all instances of a batch take the same
+ * number of z-steps.  The reference runs one instance per process (cuOPO3D.sh:65-86
+ * sweeps by re-running the binary); this is the batched replacement of that loop.
+ * tuning: {threads, tile elements, first-stage radix} for the t-, x- and y-pass
+ * (opo_get_tuning layout), or NULL for the defaults. */
+typedef struct OpoBatch OpoBatch;
+int opo_batch_create(int precision, int capacity, size_t hbm_budget_bytes, const int tuning[9], OpoBatch **out);
+void opo_batch_destroy(OpoBatch *b);
+/* Admit one instance (OPO_ERR_CAPACITY when no slot or budget is left). */
+int opo_batch_add(OpoBatch *b, const OpoParams *p, const double *w, int *slot);
+int opo_batch_remove(OpoBatch *b, int slot);
+int opo_batch_set_field(OpoBatch *b, int slot, int which, const void *src, int where, int elem_precision);
+int opo_batch_get_field(OpoBatch *b, int slot, int which, void *dst, int where, int elem_precision);
+/* Initialise a slot's fields on the device from its configuration: Api = Ap = the pump
+ * of opo_pump_field, As = opo_noise(seed, sigma), Ai = 0 (or As when idler_copy). */
+int opo_batch_init_fields(OpoBatch *b, int slot, const OpoConfig *cfg, uint64_t seed, double sigma, int idler_copy);
+/* n round trips of every admitted instance (each continues its own round-trip count). */
+int opo_batch_run_round_trips(OpoBatch *b, int n);
+/* FP64 sums of |A|^2 of pump, signal, idler for every slot: sums[3 * slot + k]
+ * (zero for empty slots); one batched reduction. */
+int opo_batch_sums(OpoBatch *b, double *sums);
+/* Slot info: {round trips done, round trips of its run, voxels, device bytes charged}. */
+int opo_batch_info(const OpoBatch *b, int slot, long long out[4]);
+/* Batch info: {admitted instances, bytes charged, budget, kernel launches}. */
+int opo_batch_stats(const OpoBatch *b, long long out[4]);
+int opo_batch_get_stream(const OpoBatch *b, void **stream);
+int opo_batch_synchronize(OpoBatch *b);
+const char *opo_batch_last_error(const OpoBatch *b);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,171 @@
+"""Batched form (opo_batch_*): many instances with uneven grids and parameters advanced
+by one persistent launch per pass.  Every slot must give exactly what a standalone
+solver with the same kernel configuration gives (bit-identical: the same kernels run
+the same arithmetic on the slot's tiles), be the same alone and mixed with others, and
+match the FP64 oracle; admission respects the HBM budget; slots can leave and join
+between round trips."""
+import numpy as np
+import pytest
+
+import cuopo3d_b200 as co
+from golden_cases import rel_l2
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+TUNING = {"t": dict(threads=128, tile=1024, r1=4), "x": dict(threads=128, tile=1024, r1=8),
+          "y": dict(threads=128, tile=1024, r1=8)}
+
+BASE = dict(nz=5, LX=300.0, LY=300.0, Lcr=3000.0, FWHM=3.0, t_window=25.0, pump_mode="focused-pulsed",
+            total_rt=3, precision=co.FP64)
+INSTANCES = [
+    dict(nx=16, ny=16, nt=32, P=300.0, w0=40.0, gdd_gamma=1.0),
+    dict(nx=32, ny=16, nt=64, P=150.0, w0=60.0, detuning=0.7, Rs=0.9),
+    dict(nx=24, ny=24, nt=48, P=500.0, w0=35.0, detuning=-1.2),
+    dict(nx=32, ny=32, nt=96, P=80.0, w0=50.0, gdd_gamma=0.5, flags=co.DISPERSION | co.DIFFRACTION | co.PHYSICS,
+         Lambda=6.5),
+]
+
+
+def cfg_of(inst, **over):
+    kw = dict(BASE)
+    kw.update(inst)
+    kw.update(over)
+    return co.make_config(**kw)
+
+
+def seed_of(k):
+    return 100 + k
+
+
+def run_solo(cfg, seed, nrt):
+    params, _ = co.derive(cfg)
+    _, w = co.time_freq(cfg.nt, params.t_window)
+    sim = co.Simulation(params, w)
+    sim.set_tuning(TUNING)
+    sim.init_fields(cfg, seed, 0.02, idler_copy=True)
+    sim.run_round_trips(nrt)
+    return [sim.get_field(k) for k in (co.FIELD_AP, co.FIELD_AS, co.FIELD_AI)]
+
+
+def make_batch(cap=8, budget=8 << 30):
+    return co.Batch(co.FP64, cap, budget, tuning=TUNING)
+
+
+def test_device_init_matches_host_pump_and_noise():
+    cfg = cfg_of(INSTANCES[2])
+    params, _ = co.derive(cfg)
+    _, w = co.time_freq(cfg.nt, params.t_window)
+    sim = co.Simulation(params, w)
+    sim.init_fields(cfg, 7, 0.02)
+    api = sim.get_field(co.FIELD_API)
+    assert rel_l2(api, co.pump_field(cfg)) < 1e-13
+    s = sim.get_field(co.FIELD_AS)
+    assert np.array_equal(s.ravel(), co.noise(7, 0.02, s.size))
+    assert not np.any(sim.get_field(co.FIELD_AI))
+
+
+def test_batch_slots_equal_standalone_and_oracle():
+    b = make_batch()
+    slots = []
+    for k, inst in enumerate(INSTANCES):
+        cfg = cfg_of(inst)
+        s = b.add(cfg)
+        b.init_fields(s, cfg, seed_of(k), 0.02, idler_copy=True)
+        slots.append((s, cfg))
+    b.run_round_trips(3)
+    for k, (s, cfg) in enumerate(slots):
+        got = [b.get_field(s, w) for w in (co.FIELD_AP, co.FIELD_AS, co.FIELD_AI)]
+        solo = run_solo(cfg, seed_of(k), 3)
+        for a, c in zip(got, solo):
+            assert np.array_equal(a, c)
+        # FP64 oracle on the same inputs
+        kw = dict(BASE)
+        kw.update(INSTANCES[k])
+        kw.pop("precision")
+        st = po.Setup(po.make_phys(**kw))
+        api = st.api_complex()
+        s0 = co.noise(seed_of(k), 0.02, api.size).reshape(api.shape)
+        ref = po.round_trips(st, api, api, s0, s0, 3)
+        for a, c in zip(got, ref):
+            assert rel_l2(a, c) < 1e-10
+
+
+def test_instance_alone_equals_instance_in_mix():
+    cfg = cfg_of(INSTANCES[1])
+    b1 = make_batch()
+    s1 = b1.add(cfg)
+    b1.init_fields(s1, cfg, 5, 0.02, idler_copy=True)
+    b1.run_round_trips(2)
+    alone = b1.get_field(s1, co.FIELD_AS)
+    b2 = make_batch()
+    for k in (0, 2, 3):
+        c = cfg_of(INSTANCES[k])
+        s = b2.add(c)
+        b2.init_fields(s, c, seed_of(k), 0.02)
+    s2 = b2.add(cfg)
+    b2.init_fields(s2, cfg, 5, 0.02, idler_copy=True)
+    b2.run_round_trips(2)
+    assert np.array_equal(alone, b2.get_field(s2, co.FIELD_AS))
+
+
+def test_admission_respects_budget_and_slots():
+    cfg = cfg_of(INSTANCES[3])
+    b = co.Batch(co.FP64, 2, 1 << 20, tuning=TUNING)  # 1 MiB: nothing fits
+    with pytest.raises(co.OpoError) as e:
+        b.add(cfg)
+    assert e.value.code == co.OPO_ERR_CAPACITY
+    b = co.Batch(co.FP64, 1, 8 << 30, tuning=TUNING)
+    b.add(cfg)
+    with pytest.raises(co.OpoError) as e:
+        b.add(cfg)
+    assert e.value.code == co.OPO_ERR_CAPACITY
+    st = b.stats()
+    assert st["instances"] == 1 and st["used"] <= st["budget"]
+
+
+def test_slots_leave_and_join_between_round_trips():
+    b = make_batch()
+    ca, cb, cc = cfg_of(INSTANCES[0]), cfg_of(INSTANCES[1]), cfg_of(INSTANCES[2])
+    sa = b.add(ca)
+    b.init_fields(sa, ca, 1, 0.02, idler_copy=True)
+    sb = b.add(cb)
+    b.init_fields(sb, cb, 2, 0.02, idler_copy=True)
+    b.run_round_trips(1)
+    b.remove(sb)
+    sc = b.add(cc)
+    b.init_fields(sc, cc, 3, 0.02, idler_copy=True)
+    b.run_round_trips(2)
+    assert b.info(sa)["round_trips"] == 3 and b.info(sc)["round_trips"] == 2
+    assert np.array_equal(b.get_field(sa, co.FIELD_AS), run_solo(ca, 1, 3)[1])
+    assert np.array_equal(b.get_field(sc, co.FIELD_AS), run_solo(cc, 3, 2)[1])
+
+
+def test_per_slot_last_round_trip_and_tallies():
+    """Slots with different run lengths: each skips the free-space return on its own last
+    round trip (Solver3D.cuh:987); batched FP64 tallies equal the per-field sums."""
+    b = make_batch()
+    ca = cfg_of(INSTANCES[0], total_rt=2)
+    cb = cfg_of(INSTANCES[1], total_rt=4)
+    sa = b.add(ca)
+    b.init_fields(sa, ca, 1, 0.02, idler_copy=True)
+    sb = b.add(cb)
+    b.init_fields(sb, cb, 2, 0.02, idler_copy=True)
+    b.run_round_trips(2)
+    fa = b.get_field(sa, co.FIELD_AS)
+    assert np.array_equal(fa, run_solo(ca, 1, 2)[1])
+    b.remove(sa)
+    b.run_round_trips(2)
+    fields = [b.get_field(sb, w) for w in (co.FIELD_AP, co.FIELD_AS, co.FIELD_AI)]
+    assert np.array_equal(fields[1], run_solo(cb, 2, 4)[1])
+    sums = b.sums()
+    for k in range(3):
+        ref = float(np.sum(np.abs(fields[k]) ** 2))
+        assert abs(sums[sb, k] - ref) <= 1e-12 * ref
+    assert np.all(sums[sa] == 0)
+
+
+def test_incompatible_grid_rejected():
+    b = make_batch()
+    with pytest.raises(co.OpoError):
+        b.add(cfg_of(dict(nx=12, ny=12, nt=24, P=10.0, w0=40.0)))  # 12 has no radix-8 first stage
