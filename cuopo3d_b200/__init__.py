@@ -103,6 +103,7 @@ def lib():
         L.opo_batch_synchronize.argtypes = [vp]
         L.opo_batch_last_error.argtypes = [vp]
         L.opo_batch_last_error.restype = ctypes.c_char_p
+        L.opo_serve.argtypes = [vp, _i, vp, vp, dp]
         L.opo_autotune.argtypes = [vp]
         L.opo_get_tuning.argtypes = [vp, ctypes.POINTER(_i)]
         L.opo_set_tuning.argtypes = [vp, ctypes.POINTER(_i)]
@@ -287,6 +288,55 @@ class Simulation:
             self.close()
         except Exception:
             pass
+
+
+class OpoServeRequest(ctypes.Structure):
+    _fields_ = [("cfg", OpoConfig), ("arrival_s", _d), ("seed", ctypes.c_uint64), ("noise_sigma", _d),
+                ("tol", _d)]
+
+
+class OpoServeOptions(ctypes.Structure):
+    _fields_ = [("precision", _i), ("capacity", _i), ("hbm_budget", ctypes.c_size_t), ("realtime", _i),
+                ("tuning_set", _i), ("tuning", _i * 9)]
+
+
+class OpoServeResult(ctypes.Structure):
+    _fields_ = [("status", _i), ("round_trips", _i), ("admit_s", _d), ("done_s", _d), ("latency_s", _d),
+                ("power", _d * 3), ("voxel_steps", ctypes.c_longlong)]
+
+
+SERVE_STATS = ("p50_latency_s", "p99_latency_s", "wall_s", "voxel_steps_per_s", "max_resident",
+               "kernel_launches", "voxel_steps", "completed")
+
+
+def serve(requests, precision, capacity, hbm_budget, realtime=True, tuning=None):
+    """Run a request stream with continuous batching (opo_serve).  requests: list of
+    dicts with cfg (OpoConfig), arrival_s, seed, noise_sigma, tol.  Returns (results, stats)."""
+    n = len(requests)
+    reqs = (OpoServeRequest * max(n, 1))()
+    for k, r in enumerate(requests):
+        reqs[k].cfg = r["cfg"]
+        reqs[k].arrival_s = r.get("arrival_s", 0.0)
+        reqs[k].seed = r.get("seed", 1)
+        reqs[k].noise_sigma = r.get("noise_sigma", 1e-6)
+        reqs[k].tol = r.get("tol", 0.0)
+    opt = OpoServeOptions()
+    opt.precision, opt.capacity, opt.hbm_budget, opt.realtime = precision, capacity, int(hbm_budget), int(realtime)
+    if tuning is not None:
+        opt.tuning_set = 1
+        flat = []
+        for k in ("t", "x", "y"):
+            flat += [tuning[k]["threads"], tuning[k]["tile"], tuning[k]["r1"]]
+        opt.tuning = (_i * 9)(*flat)
+    out = (OpoServeResult * max(n, 1))()
+    stats = np.zeros(8)
+    rc = lib().opo_serve(reqs, n, ctypes.byref(opt), out, _dptr(stats))
+    if rc:
+        raise OpoError(rc, lib().opo_batch_last_error(None).decode())
+    res = [dict(status=o.status, round_trips=o.round_trips, admit_s=o.admit_s, done_s=o.done_s,
+                latency_s=o.latency_s, power=np.array(o.power[:]), voxel_steps=o.voxel_steps)
+           for o in out[:n]]
+    return res, dict(zip(SERVE_STATS, stats))
 
 
 class Batch:

@@ -261,6 +261,41 @@ int opo_batch_get_stream(const OpoBatch *b, void **stream);
 int opo_batch_synchronize(OpoBatch *b);
 const char *opo_batch_last_error(const OpoBatch *b);
 
+/* ---- served form: continuous batching of sweep requests --------------------------- */
+
+typedef struct OpoServeRequest {
+    OpoConfig cfg;        /* the instance; cfg.total_rt bounds its round trips           */
+    double arrival_s;     /* arrival time after the start of the stream                   */
+    uint64_t seed;        /* signal noise seed (opo_noise)                                */
+    double noise_sigma;   /* signal noise standard deviation per component                */
+    double tol;           /* retire when |dPs/Ps| over one round trip <= tol (<= 0: never) */
+} OpoServeRequest;
+
+typedef struct OpoServeOptions {
+    int precision;        /* OPO_FP32 / OPO_FP64 for every request                        */
+    int capacity;         /* slots (resident instances at most)                           */
+    size_t hbm_budget;    /* device bytes the resident instances may take                 */
+    int realtime;         /* 1: admit a request only once the wall clock reaches its arrival */
+    int tuning_set;       /* 1: use `tuning` for the batch kernels                        */
+    int tuning[9];
+} OpoServeOptions;
+
+typedef struct OpoServeResult {
+    int status;           /* OPO_OK, OPO_ERR_NONFINITE (fields stopped being finite),
+                             OPO_ERR_INVALID (malformed), OPO_ERR_CAPACITY (never fits)   */
+    int round_trips;
+    double admit_s, done_s, latency_s;  /* latency = done - arrival                        */
+    double power[3];      /* final FP64 sums of |A|^2 (pump, signal, idler)              */
+    long long voxel_steps;
+} OpoServeResult;
+
+/* Run a stream of requests with continuous batching (see serve.cpp): requests that
+ * arrive while others run are admitted as slots and memory free up, and all resident
+ * instances advance together one round trip at a time.  stats = {p50 latency s, p99
+ * latency s, wall s, voxel-steps/s, most resident at once, kernel launches, voxel-steps,
+ * completed}.  The reference's sweep re-runs its binary per point (cuOPO3D.sh:65-86). */
+int opo_serve(const OpoServeRequest *reqs, int n, const OpoServeOptions *opt, OpoServeResult *out, double stats[8]);
+
 #ifdef __cplusplus
 }
 #endif
