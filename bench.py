@@ -283,12 +283,83 @@ def run_ours(args):
                      "passes": out["fp32"]["passes"], "e2e": out["fp32"]["e2e"],
                      "clocks": out["fp32"]["clocks"]},
         }
+        if not args.no_forms:
+            tun = out["fp32"]["tuning"]
+            line["batched"] = batched_leg(co, tun)
+            # arrival rate at ~85 % of capacity: throughput / mean work of a request
+            mean_vox = (64 * 64 * 128 + 128 * 128 * 256 + 96 * 96 * 192) / 3.0
+            rate = 0.85 * line["batched"]["value"] / (mean_vox * 100 * 15)
+            line["served"] = served_leg(co, tun, rate)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def batched_leg(co, tuning, n_inst=64, warm=1, steps=3, seed=2024):
+    """Batched form: n_inst instances with grids drawn from N in {32, 64, 128} and
+    NT in {64, 128, 256}, P log-uniform 0.5-20 W, waist U[30, 100] um, detuning U[-pi, pi],
+    20 mm PPLN, 100 slices, FP32; one persistent launch per pass for all of them."""
+    import torch
+    rng = np.random.default_rng(seed)
+    b = co.Batch(co.FP32, n_inst, 150 << 30, tuning=tuning)
+    vox = 0
+    for k in range(n_inst):
+        N = int(rng.choice([32, 64, 128]))
+        NT = int(rng.choice([64, 128, 256]))
+        cfg = co.make_config(nx=N, ny=N, nt=NT, nz=100, LX=800.0, LY=800.0, Lcr=20000.0, t_window=40.0,
+                             P=float(np.exp(rng.uniform(np.log(0.5), np.log(20.0)))),
+                             w0=float(rng.uniform(30, 100)), detuning=float(rng.uniform(-np.pi, np.pi)),
+                             FWHM=2.0, focal=10000.0, Rs=0.98, alpha=(2e-7, 2e-7, 2e-7), zloop_f32=1,
+                             pump_mode="focused-pulsed", total_rt=200, precision=co.FP32)
+        slot = b.add(cfg)
+        b.init_fields(slot, cfg, 1000 + k, 1e-3)
+        vox += N * N * NT
+    b.run_round_trips(warm)
+    b.synchronize()
+    stream = torch.cuda.ExternalStream(b.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = b.stats()["launches"]
+    e0.record(stream)
+    b.run_round_trips(steps)
+    e1.record(stream)
+    b.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = b.stats()["launches"] - l0
+    b.close()
+    return {"value": vox * 100.0 * steps / (ms * 1e-3), "unit": UNIT, "instances": n_inst,
+            "voxels": vox, "round_trips_timed": steps, "ms_per_round_trip": ms / steps,
+            "launches_per_round_trip": launches / steps, "precision": "fp32",
+            "workload": "64 instances, N in {32,64,128}, NT in {64,128,256}, 20 mm PPLN, 100 slices"}
+
+
+def served_leg(co, tuning, rate_per_s, n_req=40, seed=7):
+    """Served form, bounded sample of the request stream: n_req Poisson arrivals at
+    rate_per_s, grids from {64^2x128, 128^2x256, 96^2x192}, P log-uniform 0.5-20 W,
+    waist U[30, 100] um, 5-25 round trips (retired early when the signal power changes by
+    less than 1e-6 over a round trip), 150 GB budget, FP32."""
+    rng = np.random.default_rng(seed)
+    grids = [(64, 128), (128, 256), (96, 192)]
+    reqs, t = [], 0.0
+    for k in range(n_req):
+        t += float(rng.exponential(1.0 / rate_per_s))
+        N, NT = grids[int(rng.integers(0, 3))]
+        cfg = co.make_config(nx=N, ny=N, nt=NT, nz=100, LX=800.0, LY=800.0, Lcr=20000.0, t_window=40.0,
+                             P=float(np.exp(rng.uniform(np.log(0.5), np.log(20.0)))),
+                             w0=float(rng.uniform(30, 100)), FWHM=2.0, focal=10000.0, Rs=0.98,
+                             alpha=(2e-7, 2e-7, 2e-7), zloop_f32=1, pump_mode="focused-pulsed",
+                             total_rt=int(rng.integers(5, 26)), precision=co.FP32)
+        reqs.append(dict(cfg=cfg, arrival_s=t, seed=5000 + k, noise_sigma=1e-3, tol=1e-6))
+    res, st = co.serve(reqs, co.FP32, capacity=1024, hbm_budget=150 << 30, realtime=True, tuning=tuning)
+    ok = sum(1 for r in res if r["status"] == co.OPO_OK)
+    return {"p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
+            "value": st["voxel_steps_per_s"], "unit": UNIT, "requests": n_req, "completed": ok,
+            "arrival_rate_per_s": rate_per_s, "wall_s": st["wall_s"], "max_resident": st["max_resident"],
+            "precision": "fp32",
+            "workload": "Poisson stream, grids {64^2x128, 128^2x256, 96^2x192}, 5-25 round trips, "
+                        "early retirement at |dPs/Ps| < 1e-6, 150 GB budget"}
 
 
 def cpu_baseline(z_steps=10):
@@ -365,6 +436,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched and served legs")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup) if args.impl == "ours" else args.warmup
     if args.impl == "reference":
