@@ -132,31 +132,20 @@ def dist_setup(n_gpus):
 
 def barrier_sync(world):
     import torch
+    from cuopo3d_b200 import shard
     torch.cuda.synchronize()
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    shard.barrier()
     torch.cuda.synchronize()
 
 
 def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from cuopo3d_b200 import shard
+    return shard.reduce_scalar(x, "max")
 
 
 def sum_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    from cuopo3d_b200 import shard
+    return shard.reduce_scalar(x, "sum")
 
 
 def make_instance(co, precision, seed):
