@@ -221,7 +221,8 @@ struct PassCfg {
     size_t te = 0;
     opo::AxisPlan plan{};
     opo::TileGeom geo{};
-    size_t smem = 0;
+    size_t smem = 0;  // one tile buffer (3 field regions)
+    int grid = 0;     // CTAs of the single-instance kernel
     void *tw = nullptr;
     void *tab[2][3] = {};
     std::vector<void *> allocs;
@@ -388,31 +389,26 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     opo::TileGeom &g = pc.geo;
     if (kind == kT) {
         const int P = largest_divisor_leq(nx, (int)(te / nt));
-        g.nlines = P; g.LS = P; g.ntiles = (nx / P) * ny;
+        g.nlines = P; g.ntiles = (nx / P) * ny;
+        g.lsl = 1; g.lsj = P; g.region = (unsigned)(nt * P);
         g.tdiv = make_fastdiv(nx / P); g.tmulA = P; g.tmulB = nx; g.gs_j = nxy; g.gs_l = 1;
     } else if (kind == kY) {
         const int Py = largest_divisor_leq(nx, (int)(te / ny));
-        g.nlines = Py; g.LS = Py; g.ntiles = (nx / Py) * nt;
+        g.nlines = Py; g.ntiles = (nx / Py) * nt;
+        g.lsl = 1; g.lsj = Py; g.region = (unsigned)(ny * Py);
         g.tdiv = make_fastdiv(nx / Py); g.tmulA = Py; g.tmulB = nxy; g.gs_j = nx; g.gs_l = 1;
     } else {
+        // x tiles: whole rows, stored row by row with an odd row stride nx + 1 so that
+        // the line-parallel middle stages (consecutive threads on consecutive rows) and
+        // the butterfly-parallel first and last stages are both bank-conflict free
         const int rows = largest_divisor_leq(ny * nt, (int)(te / nx));
-        g.nlines = rows;
-        // Pad the line stride so that the consecutive-butterfly mapping of the first
-        // and last stages is bank-conflict free: a conflict-free unit holds 128 B
-        // (16 complex64 or 8 complex128); with q' = min(nx/R1, unit) consecutive
-        // butterflies per line, LS = unit/q' mod unit makes b LS + l distinct.
-        const int unit = fp64 ? 8 : 16;
-        int qq = nx / r1;
-        if (qq > unit) qq = unit;
-        const int step = unit / qq;
-        int LS = rows;
-        while ((LS % unit) != (step % unit)) LS++;
-        g.LS = LS;
-        g.ntiles = ny * nt / rows;
+        g.nlines = rows; g.ntiles = ny * nt / rows;
+        g.lsl = (unsigned)(nx + 1); g.lsj = 1; g.region = (unsigned)(rows * (nx + 1));
         g.tdiv = make_fastdiv(1); g.tmulA = 0; g.tmulB = (unsigned)rows * nx; g.gs_j = 1; g.gs_l = nx;
     }
     g.nl = make_fastdiv((unsigned)g.nlines);
-    pc.smem = 3 * (size_t)n * g.LS * sizeof(C);
+    g.region = (g.region + 1u) & ~1u;  // keeps every field region 16-byte aligned
+    pc.smem = 3 * (size_t)g.region * sizeof(C);
     if (pc.smem > 227 * 1024) return fail(s, OPO_ERR_INVALID, "tile does not fit in shared memory");
 
     int rc;
@@ -470,6 +466,7 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
             }
         }
     }
+    pc.grid = g.ntiles;
     drop_graphs(s);
     free_pass(s->pass[kind]);
     s->pass[kind] = pc;
@@ -551,7 +548,7 @@ int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, int wh
     const PassCfg &pc = s->pass[kT];
     const opo::TPassArgs<C> a = opo::make_tpass_args<C>(s, reset_pump, n_rk4, zh, which_tab, tmask);
     PassTimer timer(s, 0);
-    OPO_CU(s, opo::launch_tpass<C>(a, pc.v, a.g.ntiles, pc.smem, s->stream), "t-pass launch");
+    OPO_CU(s, opo::launch_tpass<C>(a, pc.v, pc.grid, pc.smem, s->stream), "t-pass launch");
     s->launches++;
     return OPO_OK;
 }
@@ -561,7 +558,7 @@ template <typename C> int enqueue_axis(OpoSolver *s, int kind, int which_tab, un
     const PassCfg &pc = s->pass[kind];
     const opo::AxisArgs<C> a = opo::make_axis_args<C>(s, kind, which_tab, mask);
     PassTimer timer(s, kind);
-    OPO_CU(s, opo::launch_axis<C>(a, pc.v, kind == kX, a.g.ntiles, pc.smem, s->stream), "axis-pass launch");
+    OPO_CU(s, opo::launch_axis<C>(a, pc.v, kind == kX, pc.grid, pc.smem, s->stream), "axis-pass launch");
     s->launches++;
     return OPO_OK;
 }
@@ -747,7 +744,7 @@ template <typename C> int autotune(OpoSolver *s)
             }
     }
     TuneEntry best{key, {}, {}};
-    const size_t tes[2] = {fp64 ? 1024u : 2048u, fp64 ? 2048u : 4096u};
+    const size_t tes[3] = {fp64 ? 512u : 1024u, fp64 ? 1024u : 2048u, fp64 ? 2048u : 4096u};
     const int threads[2] = {128, 256};
     const int r1s[3] = {4, 8, 16};
     const long long launches0 = s->launches;

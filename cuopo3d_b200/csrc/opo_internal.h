@@ -43,11 +43,14 @@ struct AxisPlan {
 // Placement of one tile of lines.  Line l, element j of tile `tile` is the global
 // element  base(tile) + j * gs_j + l * gs_l  with
 //   base(tile) = (tile % tdiv) * tmulA + (tile / tdiv) * tmulB,
-// and lives in shared memory at  j * LS + l  (one such block per field).
+// and lives in shared memory at  l * lsl + j * lsj  of its field's region (`region`
+// elements per field).  t and y tiles keep the global order (lines contiguous: lsl = 1,
+// lsj = nlines); x tiles are rows stored row by row with an odd padded row stride
+// (lsj = 1, lsl = nx + 1), so every stage's accesses are bank-conflict free.
 struct TileGeom {
     int nlines;
-    int LS;
     int ntiles;
+    unsigned lsl, lsj, region;
     FastDiv tdiv;
     FastDiv nl;  // nlines
     unsigned tmulA, tmulB;

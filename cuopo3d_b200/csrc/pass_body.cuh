@@ -1,5 +1,5 @@
-// Tile bodies of the split-step passes (shared by the single-instance kernels in
-// ssfm_kernels.cu and the batched kernels in batch_kernels.cu).
+// Tile bodies of the split-step passes, shared by the single-instance kernels
+// (ssfm_kernels.cu) and the batched kernels (batch.cu).
 //
 // Every z-step of the reference (Solver3D.cuh:946-960: RK4(dz/2), dispersion,
 // diffraction, RK4(dz/2)) is executed as three passes over the resident fields, each
@@ -8,23 +8,22 @@
 //             t-axis operator: transform, times the dispersion phase, inverse transform
 //   x-pass,   the separable diffraction operator exp(-i dz 2 pi^2 (fx^2 + fy^2) / k)
 //   y-pass    = (x factor) (y factor), one axis per pass.
-// A CTA owns a tile of whole lines of one axis for all three fields: lines are staged
-// in shared memory with the line index fastest (so every stage is bank-conflict free),
-// the first transform stage is fused with the coalesced global load (and, in the
-// t-pass, with the RK4 update) and the last inverse stage with the global store.  The
-// middle stages exchange through shared memory; the last forward stage, the phase
-// multiply and the first inverse stage are one register-resident step.
+// A CTA owns a tile of whole lines of one axis for all three fields, staged in shared
+// memory (TileGeom gives the layout).  The first forward stage reads global memory
+// directly into registers (in the t-pass it also applies the RK4 half steps), the middle
+// stages exchange through shared memory, the last forward stage, the phase multiply and
+// the first inverse stage are one register step, and the last inverse stage writes
+// global memory directly.
 //
 // Index arithmetic is 32-bit (a field holds fewer than 2^32 values) and every division
-// by a run-time invariant uses a precomputed multiply-high (FastDiv).  A tile body
-// ends with the CTA synchronised unless it staged nothing in shared memory.
+// by a run-time invariant uses a precomputed multiply-high (FastDiv).  Field f of a tile
+// lives in shared-memory region f.  Every body ends with the CTA synchronised.
 #pragma once
 
 #include "fft_radix.cuh"
 #include "opo_internal.h"
 
 namespace opo {
-
 
 template <int S, typename C> __device__ __forceinline__ C twmul(C x, C w)
 {
@@ -60,19 +59,20 @@ __device__ __forceinline__ int field_id(unsigned mask, int f)
 // Shared-memory stages.  Per field, work item w -> (line l fastest, butterfly b).
 
 template <typename C, int R, int S, bool DIT, int THREADS>
-__device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv &fq, const C *tw, int nf)
+__device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv &fq, const C *tw, unsigned mask)
 {
-    const unsigned q = fq.d, nl = (unsigned)g.nlines, LS = (unsigned)g.LS;
+    const unsigned q = fq.d, nl = (unsigned)g.nlines, lsl = g.lsl, lsj = g.lsj;
     const unsigned items = (unsigned)(n / R) * nl;
+    const int nf = __popc(mask);
     for (int f = 0; f < nf; f++) {
-        C *sf = sm + (size_t)f * n * LS;
+        C *sf = sm + (size_t)field_id(mask, f) * g.region;
         for (unsigned w = threadIdx.x; w < items; w += THREADS) {
             const unsigned b = fdiv(g.nl, w), l = w - b * nl;
             const unsigned gq = fdiv(fq, b), j = b - gq * q;
-            C *s = sf + (gq * L + j) * LS + l;
+            C *s = sf + l * lsl + (gq * L + j) * lsj;
             C x[R];
 #pragma unroll
-            for (int m = 0; m < R; m++) x[m] = s[m * q * LS];
+            for (int m = 0; m < R; m++) x[m] = s[m * q * lsj];
             if (DIT && q > 1) {
 #pragma unroll
                 for (int m = 1; m < R; m++) x[m] = twmul<S>(x[m], __ldg(tw + (m - 1) * q + j));
@@ -83,7 +83,7 @@ __device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv
                 for (int k = 1; k < R; k++) x[k] = twmul<S>(x[k], __ldg(tw + (k - 1) * q + j));
             }
 #pragma unroll
-            for (int k = 0; k < R; k++) s[k * q * LS] = x[k];
+            for (int k = 0; k < R; k++) s[k * q * lsj] = x[k];
         }
     }
 }
@@ -91,41 +91,43 @@ __device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv
 // Last forward stage (q = 1), phase multiply, first inverse stage, in registers.
 template <typename C, int R, int SF, int THREADS>
 __device__ void fused_middle(C *sm, const TileGeom &g, int n, const typename TabOf<C>::type *const *tab,
-                             unsigned tmask, int nf)
+                             unsigned mask)
 {
-    const unsigned nl = (unsigned)g.nlines, LS = (unsigned)g.LS;
+    const unsigned nl = (unsigned)g.nlines, lsl = g.lsl, lsj = g.lsj;
     const unsigned items = (unsigned)(n / R) * nl;
+    const int nf = __popc(mask);
     for (int f = 0; f < nf; f++) {
-        C *sf = sm + (size_t)f * n * LS;
-        const typename TabOf<C>::type *tf = tab[field_id(tmask, f)];
+        const int fid = field_id(mask, f);
+        C *sf = sm + (size_t)fid * g.region;
+        const typename TabOf<C>::type *tf = tab[fid];
         for (unsigned w = threadIdx.x; w < items; w += THREADS) {
             const unsigned g0 = fdiv(g.nl, w), l = w - g0 * nl;
-            C *s = sf + g0 * R * LS + l;
+            C *s = sf + l * lsl + g0 * R * lsj;
             const typename TabOf<C>::type *tb = tf + g0 * R;
             C x[R];
 #pragma unroll
-            for (int m = 0; m < R; m++) x[m] = s[m * LS];
+            for (int m = 0; m < R; m++) x[m] = s[m * lsj];
             dft<R, SF>(x);
 #pragma unroll
             for (int k = 0; k < R; k++) x[k] = tab_mul(x[k], __ldg(tb + k));
             dft<R, -SF>(x);
 #pragma unroll
-            for (int k = 0; k < R; k++) s[k * LS] = x[k];
+            for (int k = 0; k < R; k++) s[k * lsj] = x[k];
         }
     }
 }
 
 template <typename C, int S, bool DIT, int THREADS, int RMAX>
 __device__ void smem_stage_dispatch(int R, C *sm, const TileGeom &g, int n, int L, const FastDiv &fq,
-                                    const C *tw, int nf)
+                                    const C *tw, unsigned mask)
 {
     switch (R) {
-    case 2: smem_stage<C, 2, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf); break;
-    case 3: smem_stage<C, 3, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf); break;
-    case 4: smem_stage<C, 4, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf); break;
-    case 8: smem_stage<C, 8, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf); break;
+    case 2: smem_stage<C, 2, S, DIT, THREADS>(sm, g, n, L, fq, tw, mask); break;
+    case 3: smem_stage<C, 3, S, DIT, THREADS>(sm, g, n, L, fq, tw, mask); break;
+    case 4: smem_stage<C, 4, S, DIT, THREADS>(sm, g, n, L, fq, tw, mask); break;
+    case 8: smem_stage<C, 8, S, DIT, THREADS>(sm, g, n, L, fq, tw, mask); break;
     case 16:
-        if constexpr (RMAX >= 16) smem_stage<C, 16, S, DIT, THREADS>(sm, g, n, L, fq, tw, nf);
+        if constexpr (RMAX >= 16) smem_stage<C, 16, S, DIT, THREADS>(sm, g, n, L, fq, tw, mask);
         break;
     default: break;
     }
@@ -133,15 +135,15 @@ __device__ void smem_stage_dispatch(int R, C *sm, const TileGeom &g, int n, int 
 
 template <typename C, int SF, int THREADS, int RMAX>
 __device__ void fused_dispatch(int R, C *sm, const TileGeom &g, int n, const typename TabOf<C>::type *const *tab,
-                               unsigned tmask, int nf)
+                               unsigned mask)
 {
     switch (R) {
-    case 2: fused_middle<C, 2, SF, THREADS>(sm, g, n, tab, tmask, nf); break;
-    case 3: fused_middle<C, 3, SF, THREADS>(sm, g, n, tab, tmask, nf); break;
-    case 4: fused_middle<C, 4, SF, THREADS>(sm, g, n, tab, tmask, nf); break;
-    case 8: fused_middle<C, 8, SF, THREADS>(sm, g, n, tab, tmask, nf); break;
+    case 2: fused_middle<C, 2, SF, THREADS>(sm, g, n, tab, mask); break;
+    case 3: fused_middle<C, 3, SF, THREADS>(sm, g, n, tab, mask); break;
+    case 4: fused_middle<C, 4, SF, THREADS>(sm, g, n, tab, mask); break;
+    case 8: fused_middle<C, 8, SF, THREADS>(sm, g, n, tab, mask); break;
     case 16:
-        if constexpr (RMAX >= 16) fused_middle<C, 16, SF, THREADS>(sm, g, n, tab, tmask, nf);
+        if constexpr (RMAX >= 16) fused_middle<C, 16, SF, THREADS>(sm, g, n, tab, mask);
         break;
     default: break;
     }
@@ -151,19 +153,53 @@ __device__ void fused_dispatch(int R, C *sm, const TileGeom &g, int n, const typ
 // with the global load / store by the caller).
 template <typename C, int SF, int THREADS, int RMAX>
 __device__ void middle_stages(C *sm, const TileGeom &g, const AxisPlan &p, const C *tw,
-                              const typename TabOf<C>::type *const *tab, unsigned tmask, int nf)
+                              const typename TabOf<C>::type *const *tab, unsigned mask)
 {
     for (int s = 1; s < p.ns - 1; s++) {
         smem_stage_dispatch<C, SF, false, THREADS, RMAX>(p.radix[s], sm, g, p.n, p.len[s], p.q[s],
-                                                         tw + p.twoff[s], nf);
+                                                         tw + p.twoff[s], mask);
         __syncthreads();
     }
-    fused_dispatch<C, SF, THREADS, RMAX>(p.radix[p.ns - 1], sm, g, p.n, tab, tmask, nf);
+    fused_dispatch<C, SF, THREADS, RMAX>(p.radix[p.ns - 1], sm, g, p.n, tab, mask);
     __syncthreads();
     for (int s = p.ns - 2; s >= 1; s--) {
         smem_stage_dispatch<C, -SF, true, THREADS, RMAX>(p.radix[s], sm, g, p.n, p.len[s], p.q[s],
-                                                         tw + p.twoff[s], nf);
+                                                         tw + p.twoff[s], mask);
         __syncthreads();
+    }
+}
+
+// Last inverse stage (radix R1, stride q) of every field in mask, written to global.
+template <typename C, int R1, int SB, bool BFAST, int THREADS>
+__device__ __forceinline__ void final_stage(C *sm, const TileGeom &g, unsigned n, unsigned base, C *const *dst,
+                                            const C *tw, const FastDiv &fq0, unsigned mask)
+{
+    const unsigned q = n / R1, nl = (unsigned)g.nlines, items = q * nl;
+    const int nf = __popc(mask);
+    for (int f = 0; f < nf; f++) {
+        const int fid = field_id(mask, f);
+        const C *sf = sm + (size_t)fid * g.region;
+        C *df = dst[fid] + base;
+        for (unsigned w = threadIdx.x; w < items; w += THREADS) {
+            unsigned b, l;
+            if (BFAST) {
+                l = fdiv(fq0, w);
+                b = w - l * q;
+            } else {
+                b = fdiv(g.nl, w);
+                l = w - b * nl;
+            }
+            const C *s = sf + l * g.lsl + b * g.lsj;
+            C x[R1];
+#pragma unroll
+            for (int m = 0; m < R1; m++) x[m] = s[m * q * g.lsj];
+#pragma unroll
+            for (int m = 1; m < R1; m++) x[m] = twmul<SB>(x[m], __ldg(tw + (m - 1) * q + b));
+            dft<R1, SB>(x);
+            C *d = df + l * g.gs_l + b * g.gs_j;
+#pragma unroll
+            for (int k = 0; k < R1; k++) d[k * q * g.gs_j] = x[k];
+        }
     }
 }
 
@@ -233,24 +269,20 @@ template <typename C>
 __device__ __forceinline__ void rk4_half(const TPassArgs<C> &a, int h, C &p, C &s, C &i)
 {
     using T = typename TPassArgs<C>::T;
-    C k1p, k1s, k1i, k2p, k2s, k2i, k3p, k3s, k3i, k4p, k4s, k4i;
-    const T c1 = a.c1, c3 = a.c3;
     if (!a.use_phase) {
         rk4_half_fast(a, p, s, i);
         return;
-    } else {
-        const C *ph = a.ph[h];
-        cwe_rhs_phase(a.kappa, ph[0], p, s, i, k1p, k1s, k1i);
-        cwe_rhs_phase(a.kappa, ph[1], C{p.x + c1 * k1p.x, p.y + c1 * k1p.y},
-                      C{s.x + c1 * k1s.x, s.y + c1 * k1s.y}, C{i.x + c1 * k1i.x, i.y + c1 * k1i.y},
-                      k2p, k2s, k2i);
-        cwe_rhs_phase(a.kappa, ph[1], C{p.x + c1 * k2p.x, p.y + c1 * k2p.y},
-                      C{s.x + c1 * k2s.x, s.y + c1 * k2s.y}, C{i.x + c1 * k2i.x, i.y + c1 * k2i.y},
-                      k3p, k3s, k3i);
-        cwe_rhs_phase(a.kappa, ph[2], C{p.x + c3 * k3p.x, p.y + c3 * k3p.y},
-                      C{s.x + c3 * k3s.x, s.y + c3 * k3s.y}, C{i.x + c3 * k3i.x, i.y + c3 * k3i.y},
-                      k4p, k4s, k4i);
     }
+    C k1p, k1s, k1i, k2p, k2s, k2i, k3p, k3s, k3i, k4p, k4s, k4i;
+    const T c1 = a.c1, c3 = a.c3;
+    const C *ph = a.ph[h];
+    cwe_rhs_phase(a.kappa, ph[0], p, s, i, k1p, k1s, k1i);
+    cwe_rhs_phase(a.kappa, ph[1], C{p.x + c1 * k1p.x, p.y + c1 * k1p.y}, C{s.x + c1 * k1s.x, s.y + c1 * k1s.y},
+                  C{i.x + c1 * k1i.x, i.y + c1 * k1i.y}, k2p, k2s, k2i);
+    cwe_rhs_phase(a.kappa, ph[1], C{p.x + c1 * k2p.x, p.y + c1 * k2p.y}, C{s.x + c1 * k2s.x, s.y + c1 * k2s.y},
+                  C{i.x + c1 * k2i.x, i.y + c1 * k2i.y}, k3p, k3s, k3i);
+    cwe_rhs_phase(a.kappa, ph[2], C{p.x + c3 * k3p.x, p.y + c3 * k3p.y}, C{s.x + c3 * k3s.x, s.y + c3 * k3s.y},
+                  C{i.x + c3 * k3i.x, i.y + c3 * k3i.y}, k4p, k4s, k4i);
     const T w = a.h6;
     p.x += (k1p.x + T(2) * k2p.x + T(2) * k3p.x + k4p.x) * w;
     p.y += (k1p.y + T(2) * k2p.y + T(2) * k3p.y + k4p.y) * w;
@@ -260,77 +292,68 @@ __device__ __forceinline__ void rk4_half(const TPassArgs<C> &a, int h, C &p, C &
     i.y += (k1i.y + T(2) * k2i.y + T(2) * k3i.y + k4i.y) * w;
 }
 
+// Fields a t-pass must read and write: all three when it applies coupled-wave half
+// steps, else the transformed ones plus the pump when it is reset from its source.
+template <typename C> __device__ __forceinline__ unsigned tpass_load_mask(const TPassArgs<C> &a)
+{
+    return a.n_rk4 ? 7u : (a.tmask | (a.psrc != a.f[0] ? 1u : 0u));
+}
+
 // ---------------------------------------------------------------------------------
 // t-pass: tile = P consecutive pixels (x) of one row y, all t, all three fields.
-// Stage 0 (radix R1, stride q = nt/R1): each thread loads R1 time samples of one pixel
-// for p, s, i, applies n_rk4 half steps to each voxel, then the first forward stage of
-// every transformed field into shared memory (untransformed fields go straight back).
+// Stage 0 (radix R1, stride q = nt/R1): each thread takes R1 time samples of one pixel
+// for p, s, i (from global memory, or from the prefetched tile when STAGED), applies
+// n_rk4 half steps to each voxel, then the first forward stage of every transformed
+// field in place in its shared-memory region (untransformed fields go back to global).
 
 template <typename C, int R1, int THREADS, int RMAX>
 __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile, C *sm)
 {
     const AxisPlan &p = a.plan;
     const TileGeom &g = a.g;
-    const unsigned n = p.n, q = n / R1, P = g.nlines, LS = g.LS;
-    const int nf = __popc(a.tmask);
-    {
-        const unsigned base = tile_base(g, tile);
-        bool xform = nf > 0;
-        if (a.skip_rows && base >= a.nx) xform = false;  // row y = base / nx != 0
-        for (unsigned w = threadIdx.x; w < q * P; w += THREADS) {
-            const unsigned b = fdiv(g.nl, w), l = w - b * P;
-            const unsigned gb = base + l * g.gs_l + b * g.gs_j;
-            const unsigned gstep = q * g.gs_j;
-            C x[3][R1];
+    const unsigned n = p.n, q = n / R1, P = g.nlines, lsj = g.lsj;
+    const unsigned base = tile_base(g, tile);
+    bool xform = a.tmask != 0;
+    if (a.skip_rows && base >= a.nx) xform = false;  // row y = base / nx != 0
+    const unsigned tmask = xform ? a.tmask : 0u;
+    const unsigned lmask = tpass_load_mask(a);
+    for (unsigned w = threadIdx.x; w < q * P; w += THREADS) {
+        const unsigned b = fdiv(g.nl, w), l = w - b * P;
+        const unsigned gb = base + l * g.gs_l + b * g.gs_j;
+        const unsigned gstep = q * g.gs_j;
+        C x[3][R1];
 #pragma unroll
-            for (int m = 0; m < R1; m++) {
-                const unsigned gi = gb + m * gstep;
-                x[0][m] = a.psrc[gi];
-                x[1][m] = a.f[1][gi];
-                x[2][m] = a.f[2][gi];
-            }
-            for (int h = 0; h < a.n_rk4; h++) {
+        for (int f = 0; f < 3; f++) {
+            if (!(lmask & (1u << f))) continue;
+            const C *gsrc = f == 0 ? a.psrc : a.f[f];
 #pragma unroll
-                for (int m = 0; m < R1; m++) rk4_half(a, h, x[0][m], x[1][m], x[2][m]);
-            }
+            for (int m = 0; m < R1; m++)
+                x[f][m] = gsrc[gb + m * gstep];
+        }
+        for (int h = 0; h < a.n_rk4; h++) {
 #pragma unroll
-            for (int f = 0; f < 3; f++) {
-                if (xform && (a.tmask & (1u << f))) {
-                    dft<R1, +1>(x[f]);
+            for (int m = 0; m < R1; m++) rk4_half(a, h, x[0][m], x[1][m], x[2][m]);
+        }
 #pragma unroll
-                    for (int k = 1; k < R1; k++) x[f][k] = twmul<+1>(x[f][k], __ldg(a.tw + (k - 1) * q + b));
-                    C *s = sm + (size_t)__popc(a.tmask & ((1u << f) - 1u)) * n * LS + b * LS + l;
+        for (int f = 0; f < 3; f++) {
+            if (tmask & (1u << f)) {
+                dft<R1, +1>(x[f]);
 #pragma unroll
-                    for (int k = 0; k < R1; k++) s[k * q * LS] = x[f][k];
-                } else {
+                for (int k = 1; k < R1; k++) x[f][k] = twmul<+1>(x[f][k], __ldg(a.tw + (k - 1) * q + b));
+                C *s = sm + (size_t)f * g.region + l + b * lsj;
 #pragma unroll
-                    for (int m = 0; m < R1; m++) a.f[f][gb + m * gstep] = x[f][m];
-                }
+                for (int k = 0; k < R1; k++) s[k * q * lsj] = x[f][k];
+            } else if (lmask & (1u << f)) {
+#pragma unroll
+                for (int m = 0; m < R1; m++) a.f[f][gb + m * gstep] = x[f][m];
             }
         }
-        if (!xform) return;  // nothing was staged in shared memory
-        __syncthreads();
-        middle_stages<C, +1, THREADS, RMAX>(sm, g, p, a.tw, a.tab, a.tmask, nf);
-        // Stage 0 inverse (sign -1) and store.
-        for (int f = 0; f < nf; f++) {
-            C *sf = sm + (size_t)f * n * LS;
-            C *dstf = a.f[field_id(a.tmask, f)];
-            for (unsigned w = threadIdx.x; w < q * P; w += THREADS) {
-                const unsigned b = fdiv(g.nl, w), l = w - b * P;
-                const C *s = sf + b * LS + l;
-                C x[R1];
-#pragma unroll
-                for (int m = 0; m < R1; m++) x[m] = s[m * q * LS];
-#pragma unroll
-                for (int m = 1; m < R1; m++) x[m] = twmul<-1>(x[m], __ldg(a.tw + (m - 1) * q + b));
-                dft<R1, -1>(x);
-                C *dst = dstf + base + l * g.gs_l + b * g.gs_j;
-#pragma unroll
-                for (int k = 0; k < R1; k++) dst[k * q * g.gs_j] = x[k];
-            }
-        }
-        __syncthreads();
     }
+    __syncthreads();
+    if (!tmask) return;
+    middle_stages<C, +1, THREADS, RMAX>(sm, g, p, a.tw, a.tab, tmask);
+    final_stage<C, R1, -1, false, THREADS>(sm, g, n, base, a.f, a.tw, p.q[0], tmask);
+    __syncthreads();
 }
 
 // ---------------------------------------------------------------------------------
@@ -339,70 +362,47 @@ __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile,
 // consecutive butterflies of a line (x axis, where lines are rows and the transform
 // index is the contiguous one); otherwise consecutive threads take consecutive lines.
 
-template <bool BFAST>
-__device__ __forceinline__ void axis_item(unsigned w, const FastDiv &fq, const FastDiv &fnl, unsigned &b,
-                                          unsigned &l)
-{
-    if (BFAST) {
-        l = fdiv(fq, w);
-        b = w - l * fq.d;
-    } else {
-        b = fdiv(fnl, w);
-        l = w - b * fnl.d;
-    }
-}
-
 template <typename C, int R1, bool BFAST, int THREADS, int RMAX>
 __device__ __forceinline__ void axis_tile(const AxisArgs<C> &a, unsigned tile, C *sm)
 {
     const AxisPlan &p = a.plan;
     const TileGeom &g = a.g;
-    const unsigned n = p.n, q = n / R1, NL = g.nlines, LS = g.LS;
+    const unsigned n = p.n, q = n / R1, NL = g.nlines;
     const int nf = __popc(a.tmask);
     const unsigned items = q * NL;
-    if (nf == 0) return;
-    {
-        const unsigned base = tile_base(g, tile);
-        for (int f = 0; f < nf; f++) {
-            const C *srcf = a.f[field_id(a.tmask, f)] + base;
-            C *sf = sm + (size_t)f * n * LS;
-            for (unsigned w = threadIdx.x; w < items; w += THREADS) {
-                unsigned b, l;
-                axis_item<BFAST>(w, p.q[0], g.nl, b, l);
-                const C *src = srcf + l * g.gs_l + b * g.gs_j;
-                C x[R1];
-#pragma unroll
-                for (int m = 0; m < R1; m++) x[m] = src[m * q * g.gs_j];
-                dft<R1, -1>(x);
-#pragma unroll
-                for (int k = 1; k < R1; k++) x[k] = twmul<-1>(x[k], __ldg(a.tw + (k - 1) * q + b));
-                C *s = sf + b * LS + l;
-#pragma unroll
-                for (int k = 0; k < R1; k++) s[k * q * LS] = x[k];
-            }
-        }
+    if (nf == 0) {
         __syncthreads();
-        middle_stages<C, -1, THREADS, RMAX>(sm, g, p, a.tw, a.tab, a.tmask, nf);
-        for (int f = 0; f < nf; f++) {
-            C *dstf = a.f[field_id(a.tmask, f)] + base;
-            const C *sf = sm + (size_t)f * n * LS;
-            for (unsigned w = threadIdx.x; w < items; w += THREADS) {
-                unsigned b, l;
-                axis_item<BFAST>(w, p.q[0], g.nl, b, l);
-                const C *s = sf + b * LS + l;
-                C x[R1];
-#pragma unroll
-                for (int m = 0; m < R1; m++) x[m] = s[m * q * LS];
-#pragma unroll
-                for (int m = 1; m < R1; m++) x[m] = twmul<+1>(x[m], __ldg(a.tw + (m - 1) * q + b));
-                dft<R1, +1>(x);
-                C *dst = dstf + l * g.gs_l + b * g.gs_j;
-#pragma unroll
-                for (int k = 0; k < R1; k++) dst[k * q * g.gs_j] = x[k];
-            }
-        }
-        __syncthreads();
+        return;
     }
+    const unsigned base = tile_base(g, tile);
+    for (int f = 0; f < nf; f++) {
+        const int fid = field_id(a.tmask, f);
+        const C *srcf = a.f[fid] + base;
+        C *sf = sm + (size_t)fid * g.region;
+        for (unsigned w = threadIdx.x; w < items; w += THREADS) {
+            unsigned b, l;
+            if (BFAST) {
+                l = fdiv(p.q[0], w);
+                b = w - l * q;
+            } else {
+                b = fdiv(g.nl, w);
+                l = w - b * NL;
+            }
+            C *s = sf + l * g.lsl + b * g.lsj;
+            C x[R1];
+#pragma unroll
+            for (int m = 0; m < R1; m++) x[m] = srcf[l * g.gs_l + (b + m * q) * g.gs_j];
+            dft<R1, -1>(x);
+#pragma unroll
+            for (int k = 1; k < R1; k++) x[k] = twmul<-1>(x[k], __ldg(a.tw + (k - 1) * q + b));
+#pragma unroll
+            for (int k = 0; k < R1; k++) s[k * q * g.lsj] = x[k];
+        }
+    }
+    __syncthreads();
+    middle_stages<C, -1, THREADS, RMAX>(sm, g, p, a.tw, a.tab, a.tmask);
+    final_stage<C, R1, +1, BFAST, THREADS>(sm, g, n, base, a.f, a.tw, p.q[0], a.tmask);
+    __syncthreads();
 }
 
 }  // namespace opo

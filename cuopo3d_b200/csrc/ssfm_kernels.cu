@@ -7,7 +7,9 @@
 
 namespace opo {
 
-// Single-instance kernels: the grid walks the tiles of one solver.
+// Single-instance kernels: the grid walks the tiles of one solver.  Several CTAs per SM
+// (each a tile of 3 fields in shared memory) overlap one another's global loads, the
+// shared-memory stages and the stores.
 
 template <typename C, int R1, int THREADS, int RMAX>
 __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 4 : 1) tpass_kernel(TPassArgs<C> a)
