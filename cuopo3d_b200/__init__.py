@@ -253,6 +253,17 @@ class Simulation:
         return {k: dict(threads=out[3 * i], tile=out[3 * i + 1], r1=out[3 * i + 2])
                 for i, k in enumerate(("t", "x", "y"))}
 
+    def set_plane_pass(self, cluster, threads=256, r1=8):
+        """Diffraction as one fused (x, y) plane pass on clusters of `cluster` CTAs (2, 4, 8),
+        or as separate x and y passes (cluster=0)."""
+        self._check(lib().opo_set_plane_pass(self._h, int(cluster), int(threads), int(r1)))
+
+    @property
+    def plane_pass(self):
+        out = (_i * 3)()
+        self._check(lib().opo_get_plane_pass(self._h, out))
+        return dict(cluster=out[0], threads=out[1], r1=out[2])
+
     def init_fields(self, cfg, seed, sigma, idler_copy=False):
         """Api = Ap = pump, As = seeded noise, Ai = 0 (or As), computed on the device."""
         self._check(lib().opo_init_fields(self._h, ctypes.byref(cfg), seed, sigma, 1 if idler_copy else 0))

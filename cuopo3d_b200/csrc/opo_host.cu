@@ -228,6 +228,23 @@ struct PassCfg {
     std::vector<void *> allocs;
 };
 
+// Fused (x, y) plane pass: cluster size K (0: separate x and y passes), CTA size,
+// first-stage radix of both axes, plans, geometry and tables ([0] crystal step, [1]
+// free-space return).
+struct PlaneCfg {
+    int K = 0;
+    int threads = 256;
+    int r1 = 8;
+    opo::AxisPlan px{}, py{};
+    opo::TileGeom gx{}, gy{};
+    opo::FastDiv rows{};
+    unsigned regionA = 0;
+    size_t smem = 0;
+    void *twx = nullptr, *twy = nullptr;
+    void *tabx[2][3] = {}, *taby[2][3] = {};
+    std::vector<void *> allocs;
+};
+
 }  // namespace
 
 struct OpoSolver {
@@ -240,6 +257,7 @@ struct OpoSolver {
     size_t esz = 0;  // bytes per complex element
     void *field[4] = {};  // Api, Ap, As, Ai
     PassCfg pass[3];
+    PlaneCfg plane;
     std::vector<double> w;
     double *partials = nullptr, *sums_dev = nullptr;
     int sum_blocks = 0;
@@ -318,13 +336,13 @@ template <> float4 to_c<float4>(const cd &v)
     return make_float4(hx, hy, (float)(v.real() - hx), (float)(v.imag() - hy));
 }
 
-template <typename C> int upload(OpoSolver *s, PassCfg &pc, const std::vector<cd> &h, void **out)
+template <typename C> int upload(OpoSolver *s, std::vector<void *> &allocs, const std::vector<cd> &h, void **out)
 {
     std::vector<C> tmp(h.size());
     for (size_t k = 0; k < h.size(); k++) tmp[k] = to_c<C>(h[k]);
     void *d = nullptr;
     OPO_CU(s, cudaMalloc(&d, sizeof(C) * (tmp.size() ? tmp.size() : 1)), "cudaMalloc(table)");
-    pc.allocs.push_back(d);
+    allocs.push_back(d);
     if (!tmp.empty())
         OPO_CU(s, cudaMemcpy(d, tmp.data(), sizeof(C) * tmp.size(), cudaMemcpyHostToDevice), "cudaMemcpy(table)");
     *out = d;
@@ -348,6 +366,12 @@ void free_pass(PassCfg &pc)
         for (auto &t : row) t = nullptr;
 }
 
+void free_plane(PlaneCfg &pc)
+{
+    for (auto *a : pc.allocs) cudaFree(a);
+    pc = PlaneCfg{};
+}
+
 void drop_graphs(OpoSolver *s)
 {
     for (auto &g : s->graph_rt)
@@ -355,6 +379,31 @@ void drop_graphs(OpoSolver *s)
             cudaGraphExecDestroy(g);
             g = nullptr;
         }
+}
+
+// Diffraction factor tables of the x axis (xa) or the y axis in the digit-reversed order
+// of plan pl: the propagator exp(sign L 2 pi^2 / k (fx^2 + fy^2)) of Solver3D.cuh:282-323
+// factorised as (x factor)(y factor); fx = centred(i) / (dx nx).  crys[f] is the crystal
+// step (the y factor carries exp(-alpha dz / 2)), free[f] the free-space return; the
+// 1/(nx ny) normalisation is split as 1/nx, 1/ny (shipped 1/(nx ny nt) with OPO_ASIS_Q1).
+void diffraction_tables(const OpoParams &p, bool xa, const opo::AxisPlan &pl, std::vector<cd> crys[3],
+                        std::vector<cd> free[3])
+{
+    const int n = pl.n;
+    const double q1scale = (!xa && (p.flags & OPO_ASIS_Q1)) ? 1.0 / p.nt : 1.0;
+    for (int f = 0; f < 3; f++) {
+        const double d = xa ? p.dx : p.dy;
+        const double c = 2 * kPi * kPi / p.kdiff[f] / (d * n) / (d * n);
+        crys[f].assign(n, cd(0, 0));
+        free[f].assign(n, cd(0, 0));
+        for (int pos = 0; pos < n; pos++) {
+            const double u = centred(bin_of_position(pl, pos), n);
+            cd v = std::polar(1.0, -p.dz * c * u * u) / (double)n;
+            if (!xa) v *= std::exp(-0.5 * p.alpha[f] * p.dz) * q1scale;
+            crys[f][pos] = v;
+            free[f][pos] = std::polar(1.0, p.free_len * c * u * u) / (double)n;
+        }
+    }
 }
 
 // Default variant and tile size of a pass kind: 96 KB of shared memory for the three
@@ -412,7 +461,7 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     if (pc.smem > 227 * 1024) return fail(s, OPO_ERR_INVALID, "tile does not fit in shared memory");
 
     int rc;
-    if ((rc = upload<C>(s, pc, tw, &pc.tw))) { free_pass(pc); return rc; }
+    if ((rc = upload<C>(s, pc.allocs, tw, &pc.tw))) { free_pass(pc); return rc; }
     const bool phys = (p.flags & OPO_PHYSICS) != 0;
     const opo::AxisPlan &pl = pc.plan;
     if (kind == kT) {
@@ -427,7 +476,7 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
                 if (!phys) v *= std::exp(-0.5 * p.alpha[f] * p.dz);
                 tab[pos] = v * (q2scale / nt);
             }
-            if ((rc = upload<TT>(s, pc, tab, &pc.tab[0][f]))) { free_pass(pc); return rc; }
+            if ((rc = upload<TT>(s, pc.allocs, tab, &pc.tab[0][f]))) { free_pass(pc); return rc; }
         }
         // GDD compensation exp(i w^2 GDD / 2) (Solver3D.cuh:261-277, 676) times the mirror
         // sqrt(R) e^{i phase} (Cavity3D.cuh:12-28) for resonant signal / idler, / nt
@@ -440,37 +489,110 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
                 const double wk = s->w[bin_of_position(pl, pos)];
                 tab[pos] = std::polar(1.0, 0.5 * wk * wk * p.gdd) * mirror / (double)nt;
             }
-            if ((rc = upload<TT>(s, pc, tab, &pc.tab[1][f]))) { free_pass(pc); return rc; }
+            if ((rc = upload<TT>(s, pc.allocs, tab, &pc.tab[1][f]))) { free_pass(pc); return rc; }
         }
     } else {
-        // the propagator exp(sign L 2 pi^2 / k (fx^2 + fy^2)) of Solver3D.cuh:282-323
-        // factorised as (x factor)(y factor); fx = centred(i) / (dx nx).  The crystal y
-        // factor carries exp(-alpha dz / 2); the 1/(nx ny) normalisation is split as 1/nx,
-        // 1/ny (shipped 1/(nx ny nt) with OPO_ASIS_Q1).
-        const bool xa = kind == kX;
-        const double q1scale = (!xa && (p.flags & OPO_ASIS_Q1)) ? 1.0 / nt : 1.0;
-        for (int f = 0; f < 3; f++) {
-            const double d = xa ? p.dx : p.dy;
-            const double c = 2 * kPi * kPi / p.kdiff[f] / (d * n) / (d * n);
-            std::vector<cd> crys(n), free(n);
-            for (int pos = 0; pos < n; pos++) {
-                const double u = centred(bin_of_position(pl, pos), n);
-                cd v = std::polar(1.0, -p.dz * c * u * u) / (double)n;
-                if (!xa) v *= std::exp(-0.5 * p.alpha[f] * p.dz) * q1scale;
-                crys[pos] = v;
-                free[pos] = std::polar(1.0, p.free_len * c * u * u) / (double)n;
-            }
-            if ((rc = upload<TT>(s, pc, crys, &pc.tab[0][f])) || (rc = upload<TT>(s, pc, free, &pc.tab[1][f]))) {
+        std::vector<cd> crys[3], free[3];
+        diffraction_tables(p, kind == kX, pl, crys, free);
+        for (int f = 0; f < 3; f++)
+            if ((rc = upload<TT>(s, pc.allocs, crys[f], &pc.tab[0][f])) ||
+                (rc = upload<TT>(s, pc.allocs, free[f], &pc.tab[1][f]))) {
                 free_pass(pc);
                 return rc;
             }
-        }
     }
     pc.grid = g.ntiles;
     drop_graphs(s);
     free_pass(s->pass[kind]);
     s->pass[kind] = pc;
     return OPO_OK;
+}
+
+// Configure the fused (x, y) plane pass with clusters of K CTAs of `threads` threads and
+// first-stage radix r1 on both axes (K = 0 selects the separate x and y passes).  A
+// configuration that does not fit (grid not divisible by K, shared memory, no cluster
+// of K resident) is refused with OPO_ERR_INVALID and leaves the current one in place.
+template <typename C> int configure_plane(OpoSolver *s, int K, int threads, int r1)
+{
+    const OpoParams &p = s->p;
+    const bool fp64 = sizeof(C) == 16;
+    using TT = typename opo::TabOf<C>::type;
+    if (K == 0) {
+        drop_graphs(s);
+        free_plane(s->plane);
+        return OPO_OK;
+    }
+    if (K != 2 && K != 4 && K != 8) return fail(s, OPO_ERR_INVALID, "plane cluster size must be 0, 2, 4 or 8");
+    if (!opo::plane_variant_compiled(threads)) return fail(s, OPO_ERR_INVALID, "plane kernel variant not compiled");
+    const int nx = p.nx, ny = p.ny;
+    if (nx % K || ny % K) return fail(s, OPO_ERR_INVALID, "nx and ny must be multiples of the plane cluster size");
+    PlaneCfg pc;
+    pc.K = K;
+    pc.threads = threads;
+    const int rmax = opo::plane_max_radix(fp64);
+    std::vector<cd> twx, twy;
+    int rx = r1, ry = r1;
+    while (rx >= 4 && (rx > rmax || !build_plan(nx, rx, rmax, pc.px, twx))) rx /= 2;
+    while (ry >= 4 && (ry > rmax || !build_plan(ny, ry, rmax, pc.py, twy))) ry /= 2;
+    if (rx < 4 || ry < 4) return fail(s, OPO_ERR_INVALID, "grid sizes must be 2^a 3^b and >= 8");
+    pc.r1 = std::max(rx, ry);
+    const int rows = ny / K, ncol = nx / K;
+    opo::TileGeom &gx = pc.gx;
+    gx.nlines = rows; gx.ntiles = 0; gx.lsl = (unsigned)(nx + 1); gx.lsj = 1;
+    gx.region = (unsigned)(rows * (nx + 1));
+    gx.nl = make_fastdiv((unsigned)rows); gx.gs_j = 1; gx.gs_l = (unsigned)nx;
+    opo::TileGeom &gy = pc.gy;
+    gy.nlines = ncol; gy.ntiles = 0; gy.lsl = 1; gy.lsj = (unsigned)ncol; gy.region = (unsigned)(ny * ncol);
+    gy.nl = make_fastdiv((unsigned)ncol); gy.gs_j = (unsigned)nx; gy.gs_l = 1;
+    pc.rows = make_fastdiv((unsigned)rows);
+    pc.regionA = (gx.region + 1u) & ~1u;  // column region 16-byte aligned
+    pc.smem = ((size_t)pc.regionA + gy.region) * sizeof(C);
+    if (pc.smem > 227 * 1024) return fail(s, OPO_ERR_INVALID, "plane slab does not fit in shared memory");
+    if (opo::plane_max_clusters<C>(threads, K, pc.smem) < 1)
+        return fail(s, OPO_ERR_INVALID, "no cluster of the plane pass can be resident");
+    int rc;
+    if ((rc = upload<C>(s, pc.allocs, twx, &pc.twx)) || (rc = upload<C>(s, pc.allocs, twy, &pc.twy))) {
+        free_plane(pc);
+        return rc;
+    }
+    std::vector<cd> crys[3], free[3];
+    diffraction_tables(p, true, pc.px, crys, free);
+    for (int f = 0; f < 3; f++)
+        if ((rc = upload<TT>(s, pc.allocs, crys[f], &pc.tabx[0][f])) ||
+            (rc = upload<TT>(s, pc.allocs, free[f], &pc.tabx[1][f]))) {
+            free_plane(pc);
+            return rc;
+        }
+    diffraction_tables(p, false, pc.py, crys, free);
+    for (int f = 0; f < 3; f++)
+        if ((rc = upload<TT>(s, pc.allocs, crys[f], &pc.taby[0][f])) ||
+            (rc = upload<TT>(s, pc.allocs, free[f], &pc.taby[1][f]))) {
+            free_plane(pc);
+            return rc;
+        }
+    drop_graphs(s);
+    free_plane(s->plane);
+    s->plane = pc;
+    return OPO_OK;
+}
+
+// Default plane pass: 256 threads, radix-8 first stages, the smallest cluster whose
+// slab leaves room for two CTAs per SM (else the largest cluster that fits); the
+// separate x and y passes when no cluster size fits the grid.
+template <typename C> int default_plane(OpoSolver *s)
+{
+    int chosen = 0;
+    for (int K : {2, 4, 8}) {
+        const size_t esz = sizeof(C);
+        if (s->p.nx % K || s->p.ny % K) continue;
+        const size_t smem = ((size_t)(s->p.ny / K) * (s->p.nx + 1) + 1 + (size_t)s->p.ny * (s->p.nx / K)) * esz;
+        if (smem > 227 * 1024) continue;
+        chosen = K;
+        if (smem <= 110 * 1024) break;
+    }
+    if (chosen && configure_plane<C>(s, chosen, 256, 8) == OPO_OK) return OPO_OK;
+    s->err.clear();
+    return configure_plane<C>(s, 0, 256, 8);
 }
 
 template <typename C> C *fld(OpoSolver *s, int k) { return static_cast<C *>(s->field[k]); }
@@ -563,6 +685,47 @@ template <typename C> int enqueue_axis(OpoSolver *s, int kind, int which_tab, un
     return OPO_OK;
 }
 
+template <typename C> int enqueue_plane(OpoSolver *s, int which_tab, unsigned mask)
+{
+    using TT = typename opo::TabOf<C>::type;
+    const PlaneCfg &pc = s->plane;
+    const OpoParams &p = s->p;
+    opo::PlaneArgs<C> a{};
+    for (int k = 0; k < 3; k++) {
+        a.f[k] = fld<C>(s, k + 1);
+        a.tabx[k] = static_cast<const TT *>(pc.tabx[which_tab][k]);
+        a.taby[k] = static_cast<const TT *>(pc.taby[which_tab][k]);
+    }
+    a.px = pc.px;
+    a.py = pc.py;
+    a.gx = pc.gx;
+    a.gy = pc.gy;
+    a.rows = pc.rows;
+    a.twx = static_cast<const C *>(pc.twx);
+    a.twy = static_cast<const C *>(pc.twy);
+    a.tmask = mask;
+    a.nx = (unsigned)p.nx;
+    a.ny = (unsigned)p.ny;
+    a.nt = (unsigned)p.nt;
+    a.K = (unsigned)pc.K;
+    a.regionA = pc.regionA;
+    const unsigned planes = (unsigned)__builtin_popcount(mask) * (unsigned)p.nt;
+    PassTimer timer(s, kX);
+    OPO_CU(s, opo::launch_plane<C>(a, pc.threads, planes, pc.smem, s->stream), "plane-pass launch");
+    s->launches++;
+    return OPO_OK;
+}
+
+// The diffraction operator of a z-step (which_tab 0) or the free-space return (1) on
+// the fields in mask: one fused plane pass, or the x then the y pass.
+template <typename C> int enqueue_diffraction(OpoSolver *s, int which_tab, unsigned mask)
+{
+    if (s->plane.K) return enqueue_plane<C>(s, which_tab, mask);
+    int rc;
+    if ((rc = enqueue_axis<C>(s, kX, which_tab, mask))) return rc;
+    return enqueue_axis<C>(s, kY, which_tab, mask);
+}
+
 // z of the first half step of step k (ref: the loop variable; physics: k dz).
 double step_z(const OpoParams &p, int k) { return k * p.dz; }
 
@@ -587,10 +750,7 @@ template <typename C> int enqueue_crystal(OpoSolver *s, bool reset_pump)
             nrk = 2;
         }
         if ((rc = enqueue_t<C>(s, reset_pump && k == 0, nrk, zh, 0, disp ? 7u : 0u))) return rc;
-        if (diff) {
-            if ((rc = enqueue_axis<C>(s, kX, 0, 7u))) return rc;
-            if ((rc = enqueue_axis<C>(s, kY, 0, 7u))) return rc;
-        }
+        if (diff && (rc = enqueue_diffraction<C>(s, 0, 7u))) return rc;
     }
     return OPO_OK;
 }
@@ -620,10 +780,7 @@ template <typename C> int enqueue_round_trip(OpoSolver *s, bool last)
     if ((rc = enqueue_crystal<C>(s, true))) return rc;
     const double z = last_half_z(p);
     if ((rc = enqueue_t<C>(s, false, 1, &z, 1, s->gdd_or_mirror ? 6u : 0u))) return rc;
-    if (!last && (p.flags & OPO_DIFFRACTION)) {
-        if ((rc = enqueue_axis<C>(s, kX, 1, 6u))) return rc;
-        if ((rc = enqueue_axis<C>(s, kY, 1, 6u))) return rc;
-    }
+    if (!last && (p.flags & OPO_DIFFRACTION) && (rc = enqueue_diffraction<C>(s, 1, 6u))) return rc;
     return OPO_OK;
 }
 
@@ -700,6 +857,7 @@ struct TuneEntry {
     TuneKey key;
     opo::PassVariant v[3];
     size_t te[3];
+    int plane[3];  // cluster size (0: separate x and y passes), threads, r1
 };
 std::mutex g_tune_mu;
 std::vector<TuneEntry> g_tune_cache;
@@ -728,6 +886,30 @@ template <typename C> int time_pass(OpoSolver *s, int kind, float *ms)
     return OPO_OK;
 }
 
+// Mean time of the diffraction operator (plane pass, or x then y pass) over 6 launches.
+template <typename C> int time_diffraction(OpoSolver *s, float *ms)
+{
+    cudaEvent_t a = nullptr, b = nullptr;
+    OPO_CU(s, cudaEventCreate(&a), "event");
+    OPO_CU(s, cudaEventCreate(&b), "event");
+    int rc = OPO_OK;
+    const int warm = 2, reps = 6;
+    for (int r = 0; r < warm + reps && !rc; r++) {
+        if (r == warm) cudaEventRecord(a, s->stream);
+        rc = enqueue_diffraction<C>(s, 0, 7u);
+    }
+    cudaEventRecord(b, s->stream);
+    cudaError_t e = cudaEventSynchronize(b);
+    float t = 0;
+    if (!rc && e == cudaSuccess) cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(s, e, "autotune timing");
+    *ms = t / reps;
+    return OPO_OK;
+}
+
 template <typename C> int autotune(OpoSolver *s)
 {
     const bool fp64 = sizeof(C) == 16;
@@ -740,10 +922,10 @@ template <typename C> int autotune(OpoSolver *s)
                     int rc = configure_pass<C>(s, k, e.v[k], e.te[k]);
                     if (rc) return rc;
                 }
-                return OPO_OK;
+                return configure_plane<C>(s, e.plane[0], e.plane[1], e.plane[2]);
             }
     }
-    TuneEntry best{key, {}, {}};
+    TuneEntry best{key, {}, {}, {0, 256, 8}};
     const size_t tes[3] = {fp64 ? 512u : 1024u, fp64 ? 1024u : 2048u, fp64 ? 2048u : 4096u};
     const int threads[2] = {128, 256};
     const int r1s[3] = {4, 8, 16};
@@ -769,6 +951,29 @@ template <typename C> int autotune(OpoSolver *s)
                 }
         int rc = configure_pass<C>(s, kind, best.v[kind], best.te[kind]);
         if (rc) return rc;
+    }
+    // diffraction: the tuned x and y passes against every plane-pass variant that fits
+    {
+        int rc = configure_plane<C>(s, 0, 256, 8);
+        if (rc) return rc;
+        float best_ms = 1e30f;
+        if ((rc = time_diffraction<C>(s, &best_ms))) return rc;
+        for (int K : {2, 4, 8})
+            for (int th : {256, 512})
+                for (int r1 : r1s) {
+                    if (configure_plane<C>(s, K, th, r1) != OPO_OK) continue;
+                    if (s->plane.r1 != r1) continue;  // plan fell back to a smaller radix
+                    float ms = 0;
+                    if ((rc = time_diffraction<C>(s, &ms))) return rc;
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best.plane[0] = K;
+                        best.plane[1] = th;
+                        best.plane[2] = r1;
+                    }
+                }
+        s->err.clear();
+        if ((rc = configure_plane<C>(s, best.plane[0], best.plane[1], best.plane[2]))) return rc;
     }
     s->launches = launches0;
     // the timed passes ran on the resident fields: leave them zeroed
@@ -976,7 +1181,8 @@ static int create_impl(const OpoParams *p, const double *w, const opo::PassVaria
         if (rc) break;
         // The attribute is per kernel function and shared by every solver of the process:
         // always allow the full 227 KB so no solver lowers it under another.
-        if ((e = opo::configure_kernels(227 * 1024)) != cudaSuccess) {
+        if ((e = opo::configure_kernels(227 * 1024)) != cudaSuccess ||
+            (e = opo::configure_plane_kernels(227 * 1024)) != cudaSuccess) {
             rc = cuda_fail(s, e, "configure kernels");
             break;
         }
@@ -991,6 +1197,10 @@ static int create_impl(const OpoParams *p, const double *w, const opo::PassVaria
             rc = p->precision == OPO_FP64 ? configure_pass<double2>(s, k, v, te) : configure_pass<float2>(s, k, v, te);
         }
         if (rc) break;
+        if (!vv) {
+            rc = p->precision == OPO_FP64 ? default_plane<double2>(s) : default_plane<float2>(s);
+            if (rc) break;
+        }
         s->gdd_or_mirror = s->p.gdd != 0 || (s->p.resonant & 6u);
         s->sum_blocks = 148 * 4;
         if ((e = cudaMalloc((void **)&s->partials, sizeof(double) * 3 * (s->sum_blocks + 1))) != cudaSuccess) {
@@ -1030,6 +1240,7 @@ void opo_destroy(OpoSolver *s)
     if (s->partials) cudaFree(s->partials);
     if (s->staging) cudaFree(s->staging);
     for (auto &pc : s->pass) free_pass(pc);
+    free_plane(s->plane);
     if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -1172,6 +1383,22 @@ int opo_get_tuning(const OpoSolver *s, int out[9])
         out[3 * k + 1] = (int)s->pass[k].te;
         out[3 * k + 2] = s->pass[k].v.r1;
     }
+    return OPO_OK;
+}
+
+int opo_set_plane_pass(OpoSolver *s, int cluster, int threads, int r1)
+{
+    if (!s) return OPO_ERR_INVALID;
+    return s->p.precision == OPO_FP64 ? configure_plane<double2>(s, cluster, threads, r1)
+                                      : configure_plane<float2>(s, cluster, threads, r1);
+}
+
+int opo_get_plane_pass(const OpoSolver *s, int out[3])
+{
+    if (!s || !out) return OPO_ERR_INVALID;
+    out[0] = s->plane.K;
+    out[1] = s->plane.K ? s->plane.threads : 0;
+    out[2] = s->plane.K ? s->plane.r1 : 0;
     return OPO_OK;
 }
 

@@ -96,6 +96,25 @@ template <typename C> struct AxisArgs {
     unsigned tmask;
 };
 
+// Fused (x, y) diffraction pass over whole (field, t) planes.  A cluster of K CTAs owns
+// one plane: CTA r first holds rows [r ny/K, (r+1) ny/K) in its slab (x geometry gx:
+// rows of nx + 1 elements) and applies the x factor to them; after a cluster barrier
+// it gathers columns [r nx/K, (r+1) nx/K) of every slab through distributed shared
+// memory into its column region (y geometry gy: lines = columns, contiguous), applies
+// the y factor and writes the columns back to global memory.
+template <typename C> struct PlaneArgs {
+    C *f[3];
+    AxisPlan px, py;
+    TileGeom gx, gy;
+    FastDiv rows;       // rows per CTA (ny / K): row -> owning CTA of the cluster
+    const C *twx, *twy;
+    const typename TabOf<C>::type *tabx[3], *taby[3];
+    unsigned tmask;     // fields transformed (one plane per field and t)
+    unsigned nx, ny, nt;
+    unsigned K;         // CTAs per plane (cluster size)
+    unsigned regionA;   // elements of the slab region (the column region follows it)
+};
+
 // Kernel variant of one pass: CTA size and first-stage radix; the largest radix any
 // stage may use follows from the precision and CTA size (max_radix()).
 struct PassVariant {
@@ -128,5 +147,15 @@ template <typename C> cudaError_t launch_sums(const C *f0, const C *f1, const C 
 cudaError_t launch_convert_d2f(const double2 *src, float2 *dst, size_t n, cudaStream_t st);
 cudaError_t launch_convert_f2d(const float2 *src, double2 *dst, size_t n, cudaStream_t st);
 cudaError_t configure_kernels(size_t max_smem);
+
+// Plane pass (plane_pass.cu).  Compiled CTA sizes: 256 and 512; the largest radix is
+// plane_max_radix().  grid = planes x K CTAs in clusters of K.
+inline int plane_max_radix(bool fp64) { return fp64 ? 8 : 16; }
+inline bool plane_variant_compiled(int threads) { return threads == 256 || threads == 512; }
+template <typename C> cudaError_t launch_plane(const PlaneArgs<C> &a, int threads, unsigned planes, size_t smem,
+                                               cudaStream_t st);
+// Clusters of K CTAs with `smem` bytes each that can be resident at once (0: none).
+template <typename C> int plane_max_clusters(int threads, int K, size_t smem);
+cudaError_t configure_plane_kernels(size_t max_smem);
 
 }  // namespace opo

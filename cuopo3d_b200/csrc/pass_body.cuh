@@ -152,7 +152,7 @@ __device__ void fused_dispatch(int R, C *sm, const TileGeom &g, int n, const typ
 // Stages 1 .. ns-1 forward, fused middle, inverse back to stage 1 (stage 0 is fused
 // with the global load / store by the caller).
 template <typename C, int SF, int THREADS, int RMAX>
-__device__ void middle_stages(C *sm, const TileGeom &g, const AxisPlan &p, const C *tw,
+__device__ __forceinline__ void middle_stages(C *sm, const TileGeom &g, const AxisPlan &p, const C *tw,
                               const typename TabOf<C>::type *const *tab, unsigned mask)
 {
     for (int s = 1; s < p.ns - 1; s++) {
@@ -302,9 +302,9 @@ template <typename C> __device__ __forceinline__ unsigned tpass_load_mask(const 
 // ---------------------------------------------------------------------------------
 // t-pass: tile = P consecutive pixels (x) of one row y, all t, all three fields.
 // Stage 0 (radix R1, stride q = nt/R1): each thread takes R1 time samples of one pixel
-// for p, s, i (from global memory, or from the prefetched tile when STAGED), applies
+// for p, s, i from global memory (only the fields it changes: tpass_load_mask), applies
 // n_rk4 half steps to each voxel, then the first forward stage of every transformed
-// field in place in its shared-memory region (untransformed fields go back to global).
+// field into its shared-memory region (untransformed fields go back to global).
 
 template <typename C, int R1, int THREADS, int RMAX>
 __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile, C *sm)

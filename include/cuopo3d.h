@@ -178,13 +178,16 @@ int opo_field_sums(OpoSolver *s, double sums[3]);
  * passes are launched one by one (round trips are not replayed as graphs) with an event
  * pair around every pass kernel.  opo_pass_times() waits for the stream, returns the
  * accumulated milliseconds and launch counts per pass kind since the last call --
- * [0] t-pass, [1] x-pass, [2] y-pass, [3] other kernels -- and resets them.
+ * [0] t-pass, [1] x-pass or fused (x, y) plane pass, [2] y-pass, [3] other kernels --
+ * and resets them.
  * No counterpart in the reference (its only timer is the wall clock, Common.cuh:74-90). */
 int opo_set_pass_timing(OpoSolver *s, int enable);
 int opo_pass_times(OpoSolver *s, double ms[4], long long counts[4]);
 
 /* Time every compiled kernel variant (CTA size, first-stage radix) and tile size of
- * the t-, x- and y-passes on this solver's grid and keep the fastest for each; results
+ * the t-, x- and y-passes on this solver's grid and keep the fastest for each, then
+ * time the tuned x + y passes against every fused plane-pass variant (cluster size,
+ * CTA size, first-stage radix) and keep the faster diffraction operator; results
  * are cached per (grid, precision, device) for the process, so later solvers of the same
  * shape reuse them without timing.  The timed passes run on the resident pump, signal
  * and idler, which are left zeroed: call it right after opo_create.  Stands in for the
@@ -199,6 +202,20 @@ int opo_set_tuning(OpoSolver *s, const int tuning[9]);
 /* Chosen configuration: for the t-, x- and y-pass in turn, {CTA threads, tile elements
  * per field, first-stage radix}.  No counterpart in the reference. */
 int opo_get_tuning(const OpoSolver *s, int out[9]);
+
+/* Diffraction operator as one fused plane pass (Solver3D.cuh:282-323 applied at :954 and
+ * on the free-space return, :987-990): a thread-block cluster of `cluster` CTAs (2, 4 or
+ * 8) per (field, t) plane holds the plane in its shared memory, applies the x factor to
+ * its rows, exchanges through distributed shared memory and applies the y factor to its
+ * columns, so the fields cross HBM once for both axes instead of twice.  cluster = 0
+ * selects the separate x and y passes.  threads: 256 or 512; r1: first-stage radix of
+ * both axes (4, 8 or 16; smaller when the plan needs it).  Fails with OPO_ERR_INVALID
+ * when nx or ny is not a multiple of the cluster size or the slab does not fit; the
+ * current configuration then stays.  Solvers start with a default plane pass where one
+ * fits.  No counterpart in the reference (one cuFFT 3-D plan per field). */
+int opo_set_plane_pass(OpoSolver *s, int cluster, int threads, int r1);
+/* {cluster size (0: separate x and y passes), threads, first-stage radix}. */
+int opo_get_plane_pass(const OpoSolver *s, int out[3]);
 
 /* The CUDA stream (a cudaStream_t, returned as void*) on which this solver enqueues all
  * of its work, so that callers can order their own work or record timing events on it.

@@ -43,6 +43,7 @@ def run_solo(cfg, seed, nrt):
     _, w = co.time_freq(cfg.nt, params.t_window)
     sim = co.Simulation(params, w)
     sim.set_tuning(TUNING)
+    sim.set_plane_pass(0)  # the batched kernels run the x and y passes
     sim.init_fields(cfg, seed, 0.02, idler_copy=True)
     sim.run_round_trips(nrt)
     return [sim.get_field(k) for k in (co.FIELD_AP, co.FIELD_AS, co.FIELD_AI)]
