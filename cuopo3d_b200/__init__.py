@@ -20,9 +20,11 @@ LIB_PATH = os.path.join(HERE, "libcuopo3d.so")
 OPO_OK, OPO_ERR_INVALID, OPO_ERR_CUDA, OPO_ERR_NOMEM, OPO_ERR_NONFINITE = 0, 1, 2, 3, 4
 OPO_ERR_COURANT, OPO_ERR_CAPACITY = 5, 6
 # flags
-DISPERSION, DIFFRACTION, PHYSICS, ASIS_Q1, ASIS_Q2 = 1, 2, 4, 8, 16
+DISPERSION, DIFFRACTION, PHYSICS, ASIS_Q1, ASIS_Q2, TOD = 1, 2, 4, 8, 16, 32
 FP32, FP64 = 0, 1
-PPLN_ID, MGOSPPLT_ID = 0, 1
+PPLN_ID, MGOSPPLT_ID, MGOPPLN_ID, ZGP_ID = 0, 1, 2, 3
+CRYSTALS = {"ppln": PPLN_ID, "mgospplt": MGOSPPLT_ID, "mgosplt": MGOSPPLT_ID, "mgoppln": MGOPPLN_ID,
+            "zgp": ZGP_ID}
 FIELD_API, FIELD_AP, FIELD_AS, FIELD_AI = 0, 1, 2, 3
 MEM_HOST, MEM_DEVICE = 0, 1
 PUMP_MODES = {"waveplane-cw": 0, "waveplane-pulsed": 1, "focused-cw": 2, "focused-pulsed": 3,
@@ -41,7 +43,8 @@ class OpoConfig(ctypes.Structure):
                 ("alpha", _d * 3), ("Lcav", _d), ("Rs", _d), ("Ri", _d), ("gdd_gamma", _d),
                 ("detuning", _d), ("P", _d), ("FWHM", _d), ("w0", _d), ("focal", _d),
                 ("pump_mode", _i), ("t_window", _d), ("flags", _u), ("zloop_f32", _i),
-                ("n_steps", _i), ("total_rt", _i), ("precision", _i), ("resonant", _u)]
+                ("n_steps", _i), ("total_rt", _i), ("precision", _i), ("resonant", _u), ("pol", _u),
+                ("eom_beta", _d), ("eom_fpm", _d)]
 
 
 class OpoParams(ctypes.Structure):
@@ -50,7 +53,7 @@ class OpoParams(ctypes.Structure):
                 ("kappa", _d * 3), ("kdiff", _d * 3), ("vinv", _d * 3), ("beta2", _d * 3),
                 ("alpha", _d * 3), ("dk", _d), ("Rs", _d), ("Ri", _d), ("detuning", _d),
                 ("gdd", _d), ("free_len", _d), ("resonant", _u), ("total_rt", _i),
-                ("t_window", _d)]
+                ("t_window", _d), ("beta3", _d * 3), ("eom_beta", _d), ("eom_fpm", _d)]
 
 
 class OpoError(RuntimeError):
@@ -73,6 +76,7 @@ def lib():
         dp = ctypes.POINTER(ctypes.c_double)
         L.opo_params_from_config.argtypes = [ctypes.POINTER(OpoConfig), ctypes.POINTER(OpoParams), dp]
         L.opo_crystal_dispersion.argtypes = [_i, _d, _d, dp]
+        L.opo_crystal_dispersion_pol.argtypes = [_i, _d, _i, _d, dp]
         L.opo_time_freq.argtypes = [_i, _d, dp, dp]
         L.opo_pump_field.argtypes = [ctypes.POINTER(OpoConfig), dp]
         L.opo_noise.argtypes = [ctypes.c_uint64, _d, ctypes.c_size_t, dp]
@@ -131,7 +135,8 @@ def make_config(**kw):
              ls=1.064, nx=16, ny=16, nt=32, nz=10, dQ=-1.0, alpha=(-1.0, -1.0, -1.0), Lcav=-1.0,
              Rs=0.98, Ri=None, gdd_gamma=0.0, detuning=0.0, P=1.0, FWHM=2.0, w0=50.0, focal=None,
              pump_mode="focused-pulsed", t_window=0.0, flags=DISPERSION | DIFFRACTION,
-             zloop_f32=0, n_steps=0, total_rt=1, precision=FP64, resonant=6)
+             zloop_f32=0, n_steps=0, total_rt=1, precision=FP64, resonant=6, pol="eeo", eom_beta=0.0,
+             eom_fpm=0.0)
     d.update(kw)
     if d["Ri"] is None:
         d["Ri"] = d["Rs"]
@@ -140,7 +145,10 @@ def make_config(**kw):
     if isinstance(d["pump_mode"], str):
         d["pump_mode"] = PUMP_MODES[d["pump_mode"]]
     if isinstance(d["crystal"], str):
-        d["crystal"] = {"ppln": PPLN_ID, "mgosplt": MGOSPPLT_ID, "mgosppl t": MGOSPPLT_ID}[d["crystal"].lower()]
+        d["crystal"] = CRYSTALS[d["crystal"].lower()]
+    if isinstance(d["pol"], str):
+        # polarisation tuple of the reference (ZGP.cuh:24), e.g. "eeo": bit f = wave f is 'e'
+        d["pol"] = sum(1 << f for f, ch in enumerate(d["pol"]) if ch == "e")
     c = OpoConfig()
     for k, v in d.items():
         if k == "alpha":

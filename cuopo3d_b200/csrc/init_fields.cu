@@ -110,9 +110,15 @@ int init_fields_device(OpoSolver *s, const OpoConfig *cfg, unsigned long long se
     ps.tau = cfg->FWHM * std::sqrt(2.0) / (2 * std::sqrt(2 * std::log(2.0)));
     const double zR = kPi * np_ * ps.w02 / cfg->lp;
     const double eta = cfg->focal / zR;
-    ps.Ap0 = std::sqrt(4 * cfg->P / (kEps0 * kC * kPi * np_ * ps.w02));
+    // 3-D peak 4P/(pi w0^2) (EFields3D.cuh:249); plane-wave 1-D 2P/(pi w0^2) (EFields1D.cuh:145-148)
+    const bool one_d = p.nx == 1 && p.ny == 1;
+    if (one_d && (cfg->pump_mode == OPO_PUMP_FOCUSED_CW || cfg->pump_mode == OPO_PUMP_FOCUSED_PULSED ||
+                  cfg->pump_mode == OPO_PUMP_FOCUSED_SECH2))
+        return solver_fail(s, OPO_ERR_INVALID, "init_fields: the 1-D solver has no focused pump");
+    const double pk = one_d ? 2.0 : 4.0;
+    ps.Ap0 = std::sqrt(pk * cfg->P / (kEps0 * kC * kPi * np_ * ps.w02));
     ps.ts = cfg->FWHM / (2 * std::acosh(std::sqrt(2.0)));
-    ps.Ap0s = std::sqrt(4 * (cfg->P * p.t_window / (2 * ps.ts)) / (kEps0 * kC * kPi * np_ * ps.w02));
+    ps.Ap0s = std::sqrt(pk * (cfg->P * p.t_window / (2 * ps.ts)) / (kEps0 * kC * kPi * np_ * ps.w02));
     ps.mxr = 1;
     ps.mxi = -eta;
     const size_t V = (size_t)p.nx * p.ny * p.nt;

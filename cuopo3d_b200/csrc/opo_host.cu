@@ -63,50 +63,105 @@ struct Sellmeier {
         const double CC = -24 * L * L * L / nn * res(L, 4);
         return AA + BB + CC;
     }
+    // The exact third derivative: differentiating n n'' = -R2 + 4 L^2 res_3 - n'^2 once
+    // more gives n''' = (12 L res_3 - 24 L^3 res_4 - 3 n' n'') / n.  (d3n above is the
+    // reference's expression, which differs from it; the reference only prints its TOD.)
+    double d3n_exact(double L) const
+    {
+        const double nn = n(L);
+        return (12 * L * res(L, 3) - 24 * L * L * L * res(L, 4) - 3 * dn(L) * d2n(L)) / nn;
+    }
     double vg(double L) const { return kC / (n(L) - L * dn(L)); }
     double gvd(double L) const { return std::pow(L, 3) * d2n(L) / (2 * kPi * kC * kC); }
-    double tod(double L) const
+    double tod_of(double L, double d3) const
     {
-        return -std::pow(L, 4) / (4 * kPi * kPi * kC * kC * kC) * (3 * d2n(L) + L * d3n(L));
+        return -std::pow(L, 4) / (4 * kPi * kPi * kC * kC * kC) * (3 * d2n(L) + L * d3);
     }
+    double tod(double L) const { return tod_of(L, d3n(L)); }              // as the reference prints it
+    double tod_exact(double L) const { return tod_of(L, d3n_exact(L)); }  // applied with OPO_TOD
 };
 
 struct CrystalModel {
-    Sellmeier s;
+    Sellmeier s[3];  // pump, signal, idler (polarisation-dependent crystals differ)
     double d33;
     double alpha[3];
+    bool qpm;        // quasi-phase matched: dk includes the grating term 2 pi / Lambda
 };
 
-bool crystal_model(int kind, double T, CrystalModel &m)
+// One index model of a crystal: `extraordinary` selects the polarisation of crystals
+// that have two (ZGP); the QPM crystals are extraordinary-only.
+bool sellmeier_of(int kind, double T, bool extraordinary, Sellmeier &m)
 {
-    if (kind == OPO_PPLN) {
-        // Jundt, congruent LiNbO3 (PPLN.cuh:100-115, 57-60): f = (T - 24.5)(T + 570.82)
+    if (kind == OPO_PPLN || kind == OPO_MGOPPLN) {
+        // n^2 = G1 + G2/(L^2 - G3^2) + G4/(L^2 - a5^2) - a6 L^2 with Gi = ai + bi f,
+        // f = (T - 24.5)(T + 570.82): Jundt for congruent LiNbO3 (PPLN.cuh:100-115), Gayer
+        // for MgO:LiNbO3 (MgOPPLN.cuh:99-117)
+        const bool mgo = kind == OPO_MGOPPLN;
         const double f = (T - 24.5) * (T + 570.82);
-        const double G3 = 0.20692 + (-0.89e-8) * f;
-        m.s.a0 = 5.35583 + 4.629e-7 * f;
-        m.s.d = -1.5334e-2;
-        m.s.nr = 2;
-        m.s.B[0] = 0.100473 + 3.862e-8 * f; m.s.C2[0] = G3 * G3;
-        m.s.B[1] = 100.0 + 2.657e-5 * f;    m.s.C2[1] = 11.34927 * 11.34927;
-        m.d33 = 25.20e-6;
-        m.alpha[0] = 0.025e-4; m.alpha[1] = 0.002e-4; m.alpha[2] = 0.002e-4;
+        const double a1 = mgo ? 5.756 : 5.35583, a2 = mgo ? 0.0983 : 0.100473, a3 = mgo ? 0.2020 : 0.20692,
+                     a4 = mgo ? 189.32 : 100.0, a5 = mgo ? 12.52 : 11.34927, a6 = mgo ? 1.32e-2 : 1.5334e-2,
+                     b1 = mgo ? 2.860e-6 : 4.629e-7, b2 = mgo ? 4.700e-8 : 3.862e-8,
+                     b3 = mgo ? 6.113e-8 : -0.89e-8, b4 = mgo ? 1.516e-4 : 2.657e-5;
+        const double G3 = a3 + b3 * f;
+        m.a0 = a1 + b1 * f;
+        m.d = -a6;
+        m.nr = 2;
+        m.B[0] = a2 + b2 * f; m.C2[0] = G3 * G3;
+        m.B[1] = a4 + b4 * f; m.C2[1] = a5 * a5;
         return true;
     }
     if (kind == OPO_MGOSPPLT) {
-        // Bruner, stoichiometric LiTaO3 (MgOsPPLT.cuh:99-110, 57-60)
+        // Bruner, stoichiometric LiTaO3 (MgOsPPLT.cuh:99-110)
         const double TK2 = std::pow(T + 273.15, 2);
         const double Cc = 0.185087 + 1.607839e-8 * TK2;
-        m.s.a0 = 4.502483;
-        m.s.d = -0.02357;
-        m.s.nr = 3;
-        m.s.B[0] = 0.007294 + 3.483933e-8 * TK2; m.s.C2[0] = Cc * Cc;
-        m.s.B[1] = 0.073423;                     m.s.C2[1] = 0.199595 * 0.199595;
-        m.s.B[2] = 0.001;                        m.s.C2[2] = 7.99724 * 7.99724;
-        m.d33 = 11.0e-6;
-        m.alpha[0] = 1.57e-4; m.alpha[1] = 0.17e-6; m.alpha[2] = 0.17e-6;
+        m.a0 = 4.502483;
+        m.d = -0.02357;
+        m.nr = 3;
+        m.B[0] = 0.007294 + 3.483933e-8 * TK2; m.C2[0] = Cc * Cc;
+        m.B[1] = 0.073423;                     m.C2[1] = 0.199595 * 0.199595;
+        m.B[2] = 0.001;                        m.C2[2] = 7.99724 * 7.99724;
+        return true;
+    }
+    if (kind == OPO_ZGP) {
+        // Zelmon, ZnGeP2 (ZGP.cuh:103-126): n^2 = A + B L^2/(L^2 - CC) + D L^2/(L^2 - E),
+        // i.e. (A + B + D) + B CC/(L^2 - CC) + D E/(L^2 - E); no temperature dependence
+        const double A = extraordinary ? 8.0929 : 8.0409, B = extraordinary ? 1.8649 : 1.68625,
+                     CC = extraordinary ? 0.41468 : 0.40824, D = extraordinary ? 0.84052 : 1.2880,
+                     E = extraordinary ? 452.05 : 611.05;
+        m.a0 = A + B + D;
+        m.d = 0;
+        m.nr = 2;
+        m.B[0] = B * CC; m.C2[0] = CC;
+        m.B[1] = D * E;  m.C2[1] = E;
         return true;
     }
     return false;
+}
+
+// pol: bit f set = wave f (pump, signal, idler) extraordinary (used by ZGP only).
+bool crystal_model(int kind, double T, unsigned pol, CrystalModel &m)
+{
+    for (int f = 0; f < 3; f++)
+        if (!sellmeier_of(kind, T, (pol >> f) & 1u, m.s[f])) return false;
+    switch (kind) {
+    case OPO_PPLN:      // PPLN.cuh:57-60
+    case OPO_MGOPPLN:   // MgOPPLN.cuh:57-60
+        m.d33 = 25.20e-6;
+        m.alpha[0] = 0.025e-4; m.alpha[1] = 0.002e-4; m.alpha[2] = 0.002e-4;
+        m.qpm = true;
+        break;
+    case OPO_MGOSPPLT:  // MgOsPPLT.cuh:57-60
+        m.d33 = 11.0e-6;
+        m.alpha[0] = 1.57e-4; m.alpha[1] = 0.17e-6; m.alpha[2] = 0.17e-6;
+        m.qpm = true;
+        break;
+    default:            // ZGP.cuh:55-58: birefringent phase matching, no grating
+        m.d33 = 75.0e-6;
+        m.alpha[0] = 1.57e-4; m.alpha[1] = 0.17e-6; m.alpha[2] = 0.17e-6;
+        m.qpm = false;
+        break;
+    }
+    return true;
 }
 
 // Step count of the reference loop `for (real_t z = 0; z <= Lcr; z += dz)`
@@ -225,6 +280,7 @@ struct PassCfg {
     int grid = 0;     // CTAs of the single-instance kernel
     void *tw = nullptr;
     void *tab[2][3] = {};
+    void *eom = nullptr;  // t-pass: EOM phase per time sample (natural order), or null
     std::vector<void *> allocs;
 };
 
@@ -362,6 +418,7 @@ void free_pass(PassCfg &pc)
     for (auto *a : pc.allocs) cudaFree(a);
     pc.allocs.clear();
     pc.tw = nullptr;
+    pc.eom = nullptr;
     for (auto &row : pc.tab)
         for (auto &t : row) t = nullptr;
 }
@@ -422,12 +479,21 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     const bool fp64 = sizeof(C) == 16;
     using TT = typename opo::TabOf<C>::type;
     if (!opo::variant_compiled(fp64, kind == kT, v)) return fail(s, OPO_ERR_INVALID, "kernel variant not compiled");
+    if (kind != kT && !(p.flags & OPO_DIFFRACTION)) {
+        // no (x, y) step: the pass never runs; keep the requested variant only
+        drop_graphs(s);
+        free_pass(s->pass[kind]);
+        s->pass[kind] = PassCfg{};
+        s->pass[kind].v = v;
+        s->pass[kind].te = te;
+        return OPO_OK;
+    }
     PassCfg pc;
     pc.v = v;
     pc.te = te;
     const int nx = p.nx, ny = p.ny, nt = p.nt;
     const int n = kind == kT ? nt : (kind == kX ? nx : ny);
-    if ((size_t)n > te) return fail(s, OPO_ERR_INVALID, "axis longer than the tile");
+    if ((size_t)n > te) te = pc.te = (size_t)n;  // a tile holds at least one whole line
     std::vector<cd> tw;
     int r1 = v.r1;
     if (fp64 && kind == kT && r1 > 8) r1 = 8;  // 3 fields x r1 complex128 live in registers
@@ -466,13 +532,15 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     const opo::AxisPlan &pl = pc.plan;
     if (kind == kT) {
         // dispersion exp(i dz w (vinv + w b2/2)) exp(-alpha dz/2) / nt (Solver3D.cuh:153-169,
-        // with the 1/nt of the inverse transform folded in)
+        // with the 1/nt of the inverse transform folded in); OPO_TOD adds w^3 b3/6 to the
+        // phase (the crystals compute b3, PPLN.cuh:73, but the reference never applies it)
         const double q2scale = (p.flags & OPO_ASIS_Q2) ? 1.0 / ((double)nx * ny) : 1.0;
         for (int f = 0; f < 3; f++) {
             std::vector<cd> tab(nt);
             for (int pos = 0; pos < nt; pos++) {
                 const double wk = s->w[bin_of_position(pl, pos)];
-                cd v = std::polar(1.0, p.dz * wk * (p.vinv[f] + 0.5 * wk * p.beta2[f]));
+                const double b3 = (p.flags & OPO_TOD) ? p.beta3[f] : 0.0;
+                cd v = std::polar(1.0, p.dz * wk * (p.vinv[f] + 0.5 * wk * p.beta2[f] + wk * wk * b3 / 6.0));
                 if (!phys) v *= std::exp(-0.5 * p.alpha[f] * p.dz);
                 tab[pos] = v * (q2scale / nt);
             }
@@ -490,6 +558,15 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
                 tab[pos] = std::polar(1.0, 0.5 * wk * wk * p.gdd) * mirror / (double)nt;
             }
             if ((rc = upload<TT>(s, pc.allocs, tab, &pc.tab[1][f]))) { free_pass(pc); return rc; }
+        }
+        if (p.eom_beta != 0) {
+            // EOM exp(i beta sin(2 pi fpm t)) on the t grid (Solver1D.cuh:63-72, t of
+            // EFields3D.cuh:322-325), natural order
+            std::vector<double> tt(nt);
+            opo_time_freq(nt, p.t_window, tt.data(), nullptr);
+            std::vector<cd> e(nt);
+            for (int k = 0; k < nt; k++) e[k] = std::polar(1.0, p.eom_beta * std::sin(2 * kPi * p.eom_fpm * tt[k]));
+            if ((rc = upload<C>(s, pc.allocs, e, &pc.eom))) { free_pass(pc); return rc; }
         }
     } else {
         std::vector<cd> crys[3], free[3];
@@ -523,6 +600,7 @@ template <typename C> int configure_plane(OpoSolver *s, int K, int threads, int 
         return OPO_OK;
     }
     if (K != 2 && K != 4 && K != 8) return fail(s, OPO_ERR_INVALID, "plane cluster size must be 0, 2, 4 or 8");
+    if (!(p.flags & OPO_DIFFRACTION)) return fail(s, OPO_ERR_INVALID, "no diffraction step to fuse");
     if (!opo::plane_variant_compiled(threads)) return fail(s, OPO_ERR_INVALID, "plane kernel variant not compiled");
     const int nx = p.nx, ny = p.ny;
     if (nx % K || ny % K) return fail(s, OPO_ERR_INVALID, "nx and ny must be multiples of the plane cluster size");
@@ -581,6 +659,7 @@ template <typename C> int configure_plane(OpoSolver *s, int K, int threads, int 
 // separate x and y passes when no cluster size fits the grid.
 template <typename C> int default_plane(OpoSolver *s)
 {
+    if (!(s->p.flags & OPO_DIFFRACTION)) return configure_plane<C>(s, 0, 256, 8);
     int chosen = 0;
     for (int K : {2, 4, 8}) {
         const size_t esz = sizeof(C);
@@ -644,6 +723,7 @@ TPassArgs<C> make_tpass_args(OpoSolver *s, bool reset_pump, int n_rk4, const dou
     }
     a.skip_rows = (p.flags & OPO_ASIS_Q2) ? 1 : 0;
     a.nx = (unsigned)p.nx;
+    a.eom = which_tab == 1 ? static_cast<const C *>(pc.eom) : nullptr;
     return a;
 }
 
@@ -934,6 +1014,7 @@ template <typename C> int autotune(OpoSolver *s)
         float best_ms = 1e30f;
         best.v[kind] = s->pass[kind].v;
         best.te[kind] = s->pass[kind].te;
+        if (kind != kT && !(s->p.flags & OPO_DIFFRACTION)) continue;
         for (size_t te : tes)
             for (int th : threads)
                 for (int r1 : r1s) {
@@ -953,7 +1034,7 @@ template <typename C> int autotune(OpoSolver *s)
         if (rc) return rc;
     }
     // diffraction: the tuned x and y passes against every plane-pass variant that fits
-    {
+    if (s->p.flags & OPO_DIFFRACTION) {
         int rc = configure_plane<C>(s, 0, 256, 8);
         if (rc) return rc;
         float best_ms = 1e30f;
@@ -985,6 +1066,8 @@ template <typename C> int autotune(OpoSolver *s)
 }
 
 bool valid_grid(int n) { return n >= 4; }
+// x / y extent: >= 4, or 1 without diffraction (the plane-wave 1-D solver)
+bool valid_extent(int n, unsigned flags) { return n >= 4 || (n == 1 && !(flags & OPO_DIFFRACTION)); }
 
 }  // namespace
 
@@ -995,44 +1078,55 @@ extern "C" {
 
 const char *opo_version(void) { return "cuopo3d-b200 0.1"; }
 
+int opo_crystal_dispersion_pol(int crystal, double T, int extraordinary, double L, double out[4])
+{
+    Sellmeier m;
+    if (!out || !sellmeier_of(crystal, T, extraordinary != 0, m) || !(L > 0)) return OPO_ERR_INVALID;
+    out[0] = m.n(L);
+    out[1] = m.vg(L);
+    out[2] = m.gvd(L);
+    // ZGP has no TOD in the reference: report the exact one
+    out[3] = crystal == OPO_ZGP ? m.tod_exact(L) : m.tod(L);
+    return OPO_OK;
+}
+
 int opo_crystal_dispersion(int crystal, double T, double L, double out[4])
 {
-    CrystalModel m;
-    if (!out || !crystal_model(crystal, T, m) || !(L > 0)) return OPO_ERR_INVALID;
-    out[0] = m.s.n(L);
-    out[1] = m.s.vg(L);
-    out[2] = m.s.gvd(L);
-    out[3] = m.s.tod(L);
-    return OPO_OK;
+    return opo_crystal_dispersion_pol(crystal, T, 1, L, out);
 }
 
 int opo_params_from_config(const OpoConfig *c, OpoParams *o, double *sc)
 {
     if (!c || !o) return OPO_ERR_INVALID;
-    if (!valid_grid(c->nx) || !valid_grid(c->ny) || !valid_grid(c->nt) || c->nz < 2) return OPO_ERR_INVALID;
+    if (!valid_extent(c->nx, c->flags) || !valid_extent(c->ny, c->flags) || !valid_grid(c->nt) || c->nz < 2)
+        return OPO_ERR_INVALID;
     if (c->precision != OPO_FP32 && c->precision != OPO_FP64) return OPO_ERR_INVALID;
     CrystalModel m;
-    if (!crystal_model(c->crystal, c->T, m)) return OPO_ERR_INVALID;
+    if (!crystal_model(c->crystal, c->T, c->pol, m)) return OPO_ERR_INVALID;
     if (!(c->lp > 0) || !(c->ls > c->lp) || !(c->Lcr > 0) || !(c->LX > 0) || !(c->LY > 0)) return OPO_ERR_INVALID;
     const double lp = c->lp, ls = c->ls, li = ls * lp / (ls - lp);  // cuOPO3D.cu:17
     const double lam[3] = {lp, ls, li};
-    double n[3], v[3], b2[3], b3[3], alpha[3];
+    double n[3], v[3], b2[3], b3[3], b3x[3], alpha[3];
     for (int f = 0; f < 3; f++) {
-        n[f] = m.s.n(lam[f]);
-        v[f] = m.s.vg(lam[f]);
-        b2[f] = m.s.gvd(lam[f]);
-        b3[f] = m.s.tod(lam[f]);
+        n[f] = m.s[f].n(lam[f]);
+        v[f] = m.s[f].vg(lam[f]);
+        b2[f] = m.s[f].gvd(lam[f]);
+        b3x[f] = m.s[f].tod_exact(lam[f]);
+        b3[f] = c->crystal == OPO_ZGP ? b3x[f] : m.s[f].tod(lam[f]);
         alpha[f] = c->alpha[f] >= 0 ? c->alpha[f] : m.alpha[f];
     }
     const double dQ = c->dQ > 0 ? c->dQ : 2.0 * m.d33 / kPi;
-    const double dx = c->LX / (c->nx - 1.0), dy = c->LY / (c->ny - 1.0), dz = c->Lcr / (c->nz - 1.0);
+    // a single pixel (1-D) has no transverse step: its pump sits at r = 0
+    const double dx = c->nx > 1 ? c->LX / (c->nx - 1.0) : 0.0, dy = c->ny > 1 ? c->LY / (c->ny - 1.0) : 0.0,
+                 dz = c->Lcr / (c->nz - 1.0);
     const bool phys = (c->flags & OPO_PHYSICS) != 0;
     // EFields3D.cuh:222-224 (and the crystal constructors): kp = 2 pi ns / lp and
     // ki = 2 pi ni / ls as shipped; corrected physics uses each wave's own n and lambda.
     const double kp = phys ? 2.0 * kPi * n[0] / lp : 2.0 * kPi * n[1] / lp;
     const double ks = 2.0 * kPi * n[1] / ls;
     const double ki = phys ? 2.0 * kPi * n[2] / li : 2.0 * kPi * n[2] / ls;
-    const double dk = kp - ks - ki - 2.0 * kPi / c->Lambda;
+    // QPM crystals subtract the grating vector (PPLN.cuh:77); ZGP does not (ZGP.cuh:76)
+    const double dk = kp - ks - ki - (m.qpm ? 2.0 * kPi / c->Lambda : 0.0);
     const double Lcav = c->Lcav > 0 ? c->Lcav : 4 * c->Lcr;
     const double trt = (Lcav + c->Lcr * (n[1] - 1)) / kC;  // Cavity3D.cuh:44
     const double dt = trt / (c->nt - 1);
@@ -1046,6 +1140,7 @@ int opo_params_from_config(const OpoConfig *c, OpoParams *o, double *sc)
     for (int f = 0; f < 3; f++) {
         o->kappa[f] = 2 * kPi * dQ / (n[f] * lam[f]);  // EFields3D.cuh:219-221
         o->beta2[f] = b2[f];
+        o->beta3[f] = b3x[f];
         o->alpha[f] = alpha[f];
     }
     o->kdiff[0] = kp; o->kdiff[1] = ks; o->kdiff[2] = ki;
@@ -1060,6 +1155,8 @@ int opo_params_from_config(const OpoConfig *c, OpoParams *o, double *sc)
     o->resonant = c->resonant;
     o->total_rt = c->total_rt > 0 ? c->total_rt : 1;
     o->t_window = c->t_window > 0 ? c->t_window : trt;
+    o->eom_beta = c->eom_beta;
+    o->eom_fpm = c->eom_fpm;
     if (sc) {
         const double vals[OPO_N_SCALARS] = {n[0], n[1], n[2], v[0], v[1], v[2], b2[0], b2[1], b2[2],
                                             b3[0], b3[1], b3[2], dQ, dk, dx, dy, dz, kp, ks, ki,
@@ -1100,12 +1197,19 @@ int opo_pump_field(const OpoConfig *c, double *Api)
     const double tau = c->FWHM * std::sqrt(2.0) / (2 * std::sqrt(2 * std::log(2.0)));
     const double zR = kPi * np_ * w02 / c->lp;
     const double eta = c->focal / zR;
-    const double Ap0 = std::sqrt(4 * P / (kEps0 * kC * kPi * np_ * w02));
+    // 3-D peak 4P/(pi w0^2) (EFields3D.cuh:249); the plane-wave 1-D solver uses the mean
+    // intensity 2P/(pi w0^2) (EFields1D.cuh:145-148) and has no focused modes
+    const bool one_d = nx == 1 && ny == 1;
+    if (one_d && (c->pump_mode == OPO_PUMP_FOCUSED_CW || c->pump_mode == OPO_PUMP_FOCUSED_PULSED ||
+                  c->pump_mode == OPO_PUMP_FOCUSED_SECH2))
+        return OPO_ERR_INVALID;
+    const double pk = one_d ? 2.0 : 4.0;
+    const double Ap0 = std::sqrt(pk * P / (kEps0 * kC * kPi * np_ * w02));
     const cd MX(1, -eta);
     // sech^2 intensity envelope (new): FWHM = 2 acosh(sqrt 2) ts; P is the window-average
     // power, so the peak power is P T / (2 ts).
     const double ts = c->FWHM / (2 * std::acosh(std::sqrt(2.0)));
-    const double Ap0s = std::sqrt(4 * (P * p.t_window / (2 * ts)) / (kEps0 * kC * kPi * np_ * w02));
+    const double Ap0s = std::sqrt(pk * (P * p.t_window / (2 * ts)) / (kEps0 * kC * kPi * np_ * w02));
     const double uX = 0.5 * nx, uY = 0.5 * ny;
     for (int it = 0; it < nt; it++) {
         const double tn = t[it] / tau;
@@ -1155,7 +1259,8 @@ static int create_impl(const OpoParams *p, const double *w, const opo::PassVaria
     *out = nullptr;
     if (!p || !w) return OPO_ERR_INVALID;
     if (p->precision != OPO_FP32 && p->precision != OPO_FP64) return OPO_ERR_INVALID;
-    if (!valid_grid(p->nx) || !valid_grid(p->ny) || !valid_grid(p->nt) || p->n_steps < 1) return OPO_ERR_INVALID;
+    if (!valid_extent(p->nx, p->flags) || !valid_extent(p->ny, p->flags) || !valid_grid(p->nt) || p->n_steps < 1)
+        return OPO_ERR_INVALID;
     OpoSolver *s = new (std::nothrow) OpoSolver();
     if (!s) return OPO_ERR_NOMEM;
     s->p = *p;

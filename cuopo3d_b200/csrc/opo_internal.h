@@ -85,6 +85,8 @@ template <typename C> struct TPassArgs {
     const C *ph_steps;  // batched passes: the ph values of every t-pass of a round trip, [tp][2][3]
     int skip_rows;      // shipped quirk: transform only row y = 0 (tiles with y != 0 skip)
     unsigned nx;        // grid width (for the row test above)
+    const C *eom;       // per time sample: exp(i beta sin(2 pi fpm t)) on signal and idler
+                        // after the half steps (closing pass of a round trip), or null
 };
 
 template <typename C> struct AxisArgs {

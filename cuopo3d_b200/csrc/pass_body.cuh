@@ -334,6 +334,14 @@ __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile,
 #pragma unroll
             for (int m = 0; m < R1; m++) rk4_half(a, h, x[0][m], x[1][m], x[2][m]);
         }
+        if (a.eom) {
+#pragma unroll
+            for (int m = 0; m < R1; m++) {
+                const C e = __ldg(a.eom + b + m * q);
+                x[1][m] = cmul(x[1][m], e);
+                x[2][m] = cmul(x[2][m], e);
+            }
+        }
 #pragma unroll
         for (int f = 0; f < 3; f++) {
             if (tmask & (1u << f)) {

@@ -1,5 +1,5 @@
 """Python mirror of the reference's classes (alfredos84/cuOPO3D src/headers): crystals
-(CrystalsBase/PPLN.cuh, MgOsPPLT.cuh), Cavity (Cavity3D.cuh), EFields (EFields3D.cuh)
+(CrystalsBase/PPLN.cuh, MgOsPPLT.cuh, MgOPPLN.cuh, ZGP.cuh), Cavity (Cavity3D.cuh), EFields (EFields3D.cuh)
 and Solver (Solver3D.cuh), with the same names, arguments and members, driving the
 CUDA library through the C-ABI.
 
@@ -13,8 +13,8 @@ import ctypes
 import numpy as np
 
 from . import (DIFFRACTION, DISPERSION, FIELD_AI, FIELD_AP, FIELD_API, FIELD_AS, FP64,
-               MGOSPPLT_ID, PPLN_ID, PUMP_MODES, OpoError, Simulation, _dptr, derive, lib,
-               make_config, noise, time_freq)
+               MGOPPLN_ID, MGOSPPLT_ID, PPLN_ID, PUMP_MODES, ZGP_ID, OpoError, Simulation, _dptr, derive,
+               lib, make_config, noise, time_freq)
 
 PI = 3.14159265358979323846
 C = 299792458 * 1E6 / 1E12          # um/ps, DtypesConsts.cuh:56
@@ -26,6 +26,8 @@ class _Crystal:
     name = None
     d33 = None
     alphas = None
+    QPM = True
+    pol_bits = 0
 
     def __init__(self, LX, LY, Lcr, T, Lambda, lp, ls, li, NX=128, NY=128, NT=256, NZ=100):
         self.LX, self.LY, self.Lcr, self.T, self.Lambda = LX, LY, Lcr, T, Lambda
@@ -38,10 +40,10 @@ class _Crystal:
         self.dz = Lcr / (NZ - 1.0)
         out = np.zeros(4)
         vals = []
-        for lam in (lp, ls, li):
-            rc = lib().opo_crystal_dispersion(self.kind, T, lam, _dptr(out))
+        for f, lam in enumerate((lp, ls, li)):
+            rc = lib().opo_crystal_dispersion_pol(self.kind, T, (self.pol_bits >> f) & 1, lam, _dptr(out))
             if rc:
-                raise OpoError(rc, "opo_crystal_dispersion")
+                raise OpoError(rc, "opo_crystal_dispersion_pol")
             vals.append(out.copy())
         (self.np, self.vp, self.b2p, self.b3p), (self.ns, self.vs, self.b2s, self.b3s), \
             (self.ni, self.vi, self.b2i, self.b3i) = vals
@@ -49,7 +51,7 @@ class _Crystal:
         self.kp = 2.0 * PI * self.ns / lp
         self.ks = 2.0 * PI * self.ns / ls
         self.ki = 2.0 * PI * self.ni / ls
-        self.dk = self.kp - self.ks - self.ki - 2.0 * PI / Lambda
+        self.dk = self.kp - self.ks - self.ki - (2.0 * PI / Lambda if self.QPM else 0.0)
 
     def getCrystalProp(self):
         print(f"Crystal name = {self.name}\n        ---> Temp = {self.T} C\n"
@@ -67,6 +69,29 @@ class MgOsPPLT(_Crystal):
     alphas = (1.57e-4, 0.17e-6, 0.17e-6)
 
 
+class MgOPPLN(_Crystal):
+    """MgO:PPLN (Gayer), CrystalsBase/MgOPPLN.cuh:20-78."""
+    kind, name, d33 = MGOPPLN_ID, "MgO:PPLN", 25.20e-6
+    alphas = (0.025e-4, 0.002e-4, 0.002e-4)
+
+
+class ZGP(_Crystal):
+    """ZnGeP2 (Zelmon), CrystalsBase/ZGP.cuh:17-80: birefringent phase matching with a
+    polarisation tuple such as ('e', 'e', 'o'); no temperature or grating period."""
+    kind, name, d33 = ZGP_ID, "ZPG", 75.0e-6
+    alphas = (1.57e-4, 0.17e-6, 0.17e-6)
+    QPM = False
+
+    def __init__(self, LX, LY, Lcr, pol, lp, ls, li, **grid):
+        self.pol = tuple(pol)
+        self.pol_bits = sum(1 << f for f, ch in enumerate(self.pol) if ch == "e")
+        super().__init__(LX, LY, Lcr, 0.0, 1.0, lp, ls, li, **grid)
+
+    def setPolarizations(self, p, s, i):
+        """ZGP.cuh:98-102: stores the tuple only; the indices keep their constructed values."""
+        self.pol = (p, s, i)
+
+
 class Cavity:
     """Ring cavity, Cavity3D.cuh:31-62."""
 
@@ -78,9 +103,15 @@ class Cavity:
         self.Lfs = Lcav - Cr.Lcr
         self.gdd, self.gamma = False, 0.0
         self.detuning = 0.0
+        self.eom, self.beta, self.fpm = False, 0.0, 0.0
 
     def setGDDCompensation(self, gamma):
         self.gdd, self.gamma = True, gamma
+
+    def setEOM(self, beta, fpm):
+        """Intracavity electro-optic modulator, Cavity1D.cuh:75-84: after each pass,
+        signal and idler x exp(i beta sin(2 pi fpm t)) (Solver1D.cuh:63-72, 467)."""
+        self.eom, self.beta, self.fpm = True, beta, fpm
 
     def getCavityProp(self):
         print(f"Set OPO cavity:\n        ---> Round trip time = {self.trt} ps\n"
@@ -126,14 +157,14 @@ def _config(Cr, Cav, A, flags=DISPERSION | DIFFRACTION, precision=FP64, total_rt
     pump = A.pump or dict(P=A.Power, FWHM=1.0, w0=A.waist, focal=Cr.Lcr / 2,
                           pump_mode="focused-cw")
     res = (2 if A.resFields[1] else 0) | (4 if A.resFields[2] else 0)
-    d = dict(crystal=Cr.kind, LX=Cr.LX, LY=Cr.LY, Lcr=Cr.Lcr, T=Cr.T, Lambda=Cr.Lambda,
+    d = dict(crystal=Cr.kind, pol=Cr.pol_bits, LX=Cr.LX, LY=Cr.LY, Lcr=Cr.Lcr, T=Cr.T, Lambda=Cr.Lambda,
              lp=Cr.lp, ls=Cr.ls, nx=Cr.NX, ny=Cr.NY, nt=Cr.NT, nz=Cr.NZ, dQ=Cr.dQ,
              alpha=(Cr.alpha_crp, Cr.alpha_crs, Cr.alpha_cri),
              t_window=A.window or 0.0, flags=flags, precision=precision,
              total_rt=total_rt, resonant=res, **pump)
     if Cav is not None:
         d.update(Lcav=Cav.Lcav, Rs=Cav.Rs, Ri=Cav.Ri, gdd_gamma=Cav.gamma if Cav.gdd else 0.0,
-                 detuning=Cav.detuning)
+                 detuning=Cav.detuning, eom_beta=Cav.beta if Cav.eom else 0.0, eom_fpm=Cav.fpm if Cav.eom else 0.0)
     d.update(kw)
     return make_config(**d)
 

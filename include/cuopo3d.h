@@ -44,12 +44,20 @@ enum {
                                   absorption once, kp/ki from their own indices       */
     OPO_ASIS_Q1 = 1u << 3,     /* shipped diffraction scale 1/(NX NY NT)
                                   (Solver3D.cuh:83,780)                                 */
-    OPO_ASIS_Q2 = 1u << 4      /* shipped dispersion on row y=0 only, scale 1/(NX NY NT)
+    OPO_ASIS_Q2 = 1u << 4,     /* shipped dispersion on row y=0 only, scale 1/(NX NY NT)
                                   (Solver3D.cuh:603,613,616,629)                        */
+    OPO_TOD = 1u << 5          /* third-order dispersion: the t-axis phase gains
+                                  dz w^3 b3 / 6 (b3 of PPLN.cuh:73 etc., which the
+                                  reference computes but never applies)                 */
 };
 
 enum { OPO_FP32 = 0, OPO_FP64 = 1 };                  /* bulk field precision          */
-enum { OPO_PPLN = 0, OPO_MGOSPPLT = 1 };               /* crystal models                */
+enum {                                                 /* crystal models (Crystals.cuh)  */
+    OPO_PPLN = 0,      /* CrystalsBase/PPLN.cuh (Jundt)                         */
+    OPO_MGOSPPLT = 1,  /* CrystalsBase/MgOsPPLT.cuh (Bruner)                    */
+    OPO_MGOPPLN = 2,   /* CrystalsBase/MgOPPLN.cuh (Gayer)                      */
+    OPO_ZGP = 3        /* CrystalsBase/ZGP.cuh (Zelmon; o/e per wave, no QPM)   */
+};
 enum {                                                 /* pump profiles                 */
     OPO_PUMP_WAVEPLANE_CW = 0,     /* EFields3D.cuh:72-85    */
     OPO_PUMP_WAVEPLANE_PULSED = 1, /* EFields3D.cuh:89-103   */
@@ -71,7 +79,9 @@ typedef struct OpoConfig {
     int crystal;                       /* OPO_PPLN / OPO_MGOSPPLT                         */
     double LX, LY, Lcr, T, Lambda;     /* um, um, um, degC, um                            */
     double lp, ls;                     /* pump, signal wavelength (um); li = ls lp/(ls-lp) */
-    int nx, ny, nt, nz;                /* grid; nz slices, dz = Lcr/(nz-1)                */
+    int nx, ny, nt, nz;                /* grid; nz slices, dz = Lcr/(nz-1); nx = ny = 1 without
+                                          OPO_DIFFRACTION is the plane-wave 1-D solver
+                                          (Solver1D.cuh), nt up to one tile per CTA     */
     double dQ;                         /* um/V; <= 0 keeps the crystal's 2 d33/pi          */
     double alpha[3];                   /* 1/um; < 0 keeps the crystal's value              */
     double Lcav, Rs, Ri;               /* cavity length (um); mirror reflectivities        */
@@ -86,6 +96,13 @@ typedef struct OpoConfig {
     int total_rt;                      /* round trips of the run (the last skips free space) */
     int precision;                     /* OPO_FP32 / OPO_FP64                               */
     unsigned resonant;                 /* bit1 signal, bit2 idler (reference resFields)     */
+    unsigned pol;                      /* bit f: wave f (pump, signal, idler) extraordinary;
+                                          ZGP only (its pol tuple, ZGP.cuh:24,49)          */
+    double eom_beta, eom_fpm;          /* intracavity electro-optic modulator, Cavity::setEOM
+                                          (Cavity1D.cuh:75-84): after the crystal, signal and
+                                          idler x exp(i beta sin(2 pi fpm t)) before GDD and
+                                          mirrors (Solver1D.cuh:63-72,467); beta 0: none;
+                                          fpm in 1/ps                                       */
 } OpoConfig;
 
 /* ---- derived solver parameters (what the split-step consumes) ------------------- */
@@ -104,6 +121,8 @@ typedef struct OpoParams {
     unsigned resonant;
     int total_rt;
     double t_window;
+    double beta3[3];   /* third-order dispersion (applied with OPO_TOD)                  */
+    double eom_beta, eom_fpm;
 } OpoParams;
 
 /* Derived scalars written by opo_params_from_config (reference names, in order):
@@ -123,8 +142,12 @@ typedef struct OpoSolver OpoSolver;
 int opo_params_from_config(const OpoConfig *cfg, OpoParams *out, double *scalars);
 
 /* Refractive index n, group velocity, GVD and TOD of a crystal at one wavelength
- * (PPLN.cuh:97-259, MgOsPPLT.cuh:96-226).  out = {n, vg, b2, b3}. */
+ * (PPLN.cuh:97-259, MgOsPPLT.cuh:96-226, MgOPPLN.cuh:97-259, ZGP.cuh:103-245; ZGP
+ * defines no TOD, its b3 here is the same derivative formula on its Sellmeier form).
+ * out = {n, vg, b2, b3}.  The extraordinary index (ZGP: pol 'e'). */
 int opo_crystal_dispersion(int crystal, double T, double lambda_um, double out[4]);
+/* The same for one polarisation (extraordinary = 0: ordinary; QPM crystals ignore it). */
+int opo_crystal_dispersion_pol(int crystal, double T, int extraordinary, double lambda_um, double out[4]);
 
 /* Time and angular-frequency grids, EFields::setTimeFreqVectors
  * (EFields3D.cuh:319-328): t = linspace(-T/2, T/2), w = 2 pi fftshift(linspace(

@@ -32,7 +32,8 @@ struct PPLNModel {
     double a1 = 5.35583, a2 = 0.100473, a3 = 0.20692, a4 = 100.0, a5 = 11.34927,
            a6 = 1.5334e-2, b1 = 4.629e-7, b2 = 3.862e-8, b3 = -0.89e-8, b4 = 2.657e-5;
     double G1, G2, G3, G4;
-    explicit PPLNModel(double T)
+    explicit PPLNModel(double T) { init(T); }
+    void init(double T)
     {
         double f = (T - 24.5) * (T + 570.82);
         G1 = a1 + b1 * f; G2 = a2 + b2 * f; G3 = a3 + b3 * f; G4 = a4 + b4 * f;
@@ -47,6 +48,17 @@ struct PPLNModel {
         return G2 / std::pow(L * L - G3 * G3, p) + G4 / std::pow(L * L - a5 * a5, p);
     }
     double res2c(double L) const { return res(L, 2) + a6; }  // (resonances(2) + a6)
+};
+
+// MgO:PPLN extraordinary index, src/headers/CrystalsBase/MgOPPLN.cuh:97-143 (Gayer): the
+// PPLN form with other coefficients.
+struct MgOPPLNModel : PPLNModel {
+    explicit MgOPPLNModel(double T) : PPLNModel(T)
+    {
+        a1 = 5.756; a2 = 0.0983; a3 = 0.2020; a4 = 189.32; a5 = 12.52; a6 = 1.32e-2;
+        b1 = 2.860e-6; b2 = 4.700e-8; b3 = 6.113e-8; b4 = 1.516e-4;
+        init(T);
+    }
 };
 
 // MgO:sPPLT index, src/headers/CrystalsBase/MgOsPPLT.cuh:96-132 (Bruner).
@@ -108,7 +120,67 @@ template <class M> struct Dispersive {
     {
         return -std::pow(L, 4) / (4 * PI * PI * C * C * C) * (3 * d2n(L) + L * d3n(L));
     }
+    // the exact TOD: d3n from a central difference of d2n (the reference's d3ndl3 is
+    // not the third derivative; it only prints that TOD)
+    double TODexact(double L) const
+    {
+        const double h = 1e-4 * L;
+        const double d3 = (d2n(L - 2 * h) - 8 * d2n(L - h) + 8 * d2n(L + h) - d2n(L + 2 * h)) / (12 * h);
+        return -std::pow(L, 4) / (4 * PI * PI * C * C * C) * (3 * d2n(L) + L * d3);
+    }
 };
+
+// ZGP ordinary / extraordinary index, src/headers/CrystalsBase/ZGP.cuh:103-226 (Zelmon):
+//   n^2 = A + B L^2/(L^2 - CC) + D L^2/(L^2 - E),  fb_p = B L^2/(L^2-CC)^p, fd_p likewise,
+//   dn/dl = -(CC fb_2 + E fd_2) / (n L),
+//   d2n/dl2 = (CC fb_3 (CC/L^2 + 3) + E fd_3 (E/L^2 + 3) - (dn/dl)^2) / n.
+// The reference has no third derivative for ZGP; TOD here differentiates d2n/dl2
+// numerically (central difference), independently of the library's closed form.
+struct ZGPModel {
+    double A, B, CC, D, E;
+    explicit ZGPModel(bool e)
+    {
+        if (e) { A = 8.0929; B = 1.8649; CC = 0.41468; D = 0.84052; E = 452.05; }
+        else { A = 8.0409; B = 1.68625; CC = 0.40824; D = 1.2880; E = 611.05; }
+    }
+    double n(double L) const { return std::sqrt(A + B * L * L / (L * L - CC) + D * L * L / (L * L - E)); }
+    double fb(double L, int p) const { return B * L * L / std::pow(L * L - CC, p); }
+    double fd(double L, int p) const { return D * L * L / std::pow(L * L - E, p); }
+    double dn(double L) const { return -(CC * fb(L, 2) + E * fd(L, 2)) / (n(L) * L); }
+    double d2n(double L) const
+    {
+        const double d1 = dn(L);
+        return (CC * fb(L, 3) * (CC / (L * L) + 3) + E * fd(L, 3) * (E / (L * L) + 3) - d1 * d1) / n(L);
+    }
+    double d3n(double L) const
+    {
+        const double h = 1e-4 * L;
+        return (d2n(L - 2 * h) - 8 * d2n(L - h) + 8 * d2n(L + h) - d2n(L + 2 * h)) / (12 * h);
+    }
+    double GV(double L) const { return C / (n(L) - L * dn(L)); }
+    double GVD(double L) const { return std::pow(L, 3) * d2n(L) / (2 * PI * C * C); }
+    double TOD(double L) const
+    {
+        return -std::pow(L, 4) / (4 * PI * PI * C * C * C) * (3 * d2n(L) + L * d3n(L));
+    }
+    double TODexact(double L) const { return TOD(L); }
+};
+
+// n, vg, b2, b3 (as the reference prints it) and the exact b3 of one index of a crystal
+// (0: ok, -2: unknown crystal).
+int crystalIndex(int crystal, double T, bool extraordinary, double L, double out[5])
+{
+    auto fill = [&](const auto &m) {
+        out[0] = m.n(L); out[1] = m.GV(L); out[2] = m.GVD(L); out[3] = m.TOD(L); out[4] = m.TODexact(L);
+    };
+    switch (crystal) {
+    case OR_PPLN: fill(Dispersive<PPLNModel>(T)); return 0;
+    case OR_MGOSPPLT: fill(Dispersive<SPPLTModel>(T)); return 0;
+    case OR_MGOPPLN: fill(Dispersive<MgOPPLNModel>(T)); return 0;
+    case OR_ZGP: fill(ZGPModel(extraordinary)); return 0;
+    default: return -2;
+    }
+}
 
 // ---------------------------------------------------------------------------------
 // FFT: mixed-radix (factors 4, 2, 3, 5, then any prime) decimation in time, written
@@ -248,12 +320,14 @@ void rk4Half(const OrParams *p, double z, cd *Ap, cd *As, cd *Ai)
 
 // Dispersion propagators, Solver3D.cuh:153-169:
 //   eiLz_f(w) = exp(i dz w (vinv_f + w b2_f / 2)) exp(-alpha_f dz / 2)
+// (OR_TOD, not in the reference: the phase gains dz w^3 b3_f / 6).
 void dispersionTable(const OrParams *p, const double *w, int f, double len, bool absorb,
                      std::vector<cd> &tab)
 {
     tab.resize(p->nt);
+    const double b3 = (p->flags & OR_TOD) ? p->beta3[f] : 0.0;
     for (int k = 0; k < p->nt; k++) {
-        tab[k] = cpxExp(len * w[k] * (p->vinv[f] + 0.5 * w[k] * p->beta2[f]));
+        tab[k] = cpxExp(len * w[k] * (p->vinv[f] + 0.5 * w[k] * p->beta2[f] + w[k] * w[k] * b3 / 6.0));
         if (absorb) tab[k] *= std::exp(-0.5 * p->alpha[f] * len);
     }
 }
@@ -460,41 +534,48 @@ void or_power_sums(int n, const double *A, double *sum_abs2)
 //   Cavity constructor   Cavity3D.cuh:42-49 (trt, dt)
 //   t/w grids            EFields3D.cuh:319-328, Common.cuh:120-128, EFields3D.cuh:58-68
 //   pump field           EFields3D.cuh:244-296 with the kernels at :72-137
+int or_crystal_dispersion(int crystal, double T, int extraordinary, double L, double out[5])
+{
+    if (!out || !(L > 0)) return -1;
+    return crystalIndex(crystal, T, extraordinary != 0, L, out);
+}
+
 int or_setup(const OrPhys *in, OrParams *o, double *sc, double *t, double *w, double *Api)
 {
     const int nx = in->nx, ny = in->ny, nt = in->nt;
-    if (nx < 2 || ny < 2 || nt < 2 || in->nz < 2) return -1;
+    // nx = ny = 1 without diffraction: the plane-wave 1-D solver (Solver1D.cuh)
+    const bool diff = (in->flags & OR_DIFFRACTION) != 0;
+    if (nx < (diff ? 2 : 1) || ny < (diff ? 2 : 1) || nt < 2 || in->nz < 2) return -1;
     const double lp = in->lp, ls = in->ls, li = ls * lp / (ls - lp);
     double n[3], v[3], b2[3], b3[3], d33, alpha[3];
     const double L3[3] = {lp, ls, li};
-    if (in->crystal == OR_PPLN) {
-        Dispersive<PPLNModel> m(in->T);
-        for (int f = 0; f < 3; f++) {
-            n[f] = m.n(L3[f]); v[f] = m.GV(L3[f]); b2[f] = m.GVD(L3[f]); b3[f] = m.TOD(L3[f]);
-        }
+    double b3x[3];
+    for (int f = 0; f < 3; f++) {
+        double q[5];
+        if (crystalIndex(in->crystal, in->T, (in->pol >> f) & 1u, L3[f], q)) return -2;
+        n[f] = q[0]; v[f] = q[1]; b2[f] = q[2]; b3[f] = q[3]; b3x[f] = q[4];
+    }
+    // d33 and absorption: PPLN.cuh:57-60, MgOPPLN.cuh:57-60, MgOsPPLT.cuh:57-60, ZGP.cuh:55-58
+    if (in->crystal == OR_PPLN || in->crystal == OR_MGOPPLN) {
         d33 = 25.20e-6;
         alpha[0] = 0.025e-4; alpha[1] = 0.002e-4; alpha[2] = 0.002e-4;
-    } else if (in->crystal == OR_MGOSPPLT) {
-        Dispersive<SPPLTModel> m(in->T);
-        for (int f = 0; f < 3; f++) {
-            n[f] = m.n(L3[f]); v[f] = m.GV(L3[f]); b2[f] = m.GVD(L3[f]); b3[f] = m.TOD(L3[f]);
-        }
-        d33 = 11.0e-6;
-        alpha[0] = 1.57e-4; alpha[1] = 0.17e-6; alpha[2] = 0.17e-6;
     } else {
-        return -2;
+        d33 = in->crystal == OR_ZGP ? 75.0e-6 : 11.0e-6;
+        alpha[0] = 1.57e-4; alpha[1] = 0.17e-6; alpha[2] = 0.17e-6;
     }
     double dQ = 2.0 * d33 / PI;
     if (in->dQ > 0) dQ = in->dQ;
     for (int f = 0; f < 3; f++)
         if (in->alpha[f] >= 0) alpha[f] = in->alpha[f];
-    const double dx = in->LX / (nx - 1.0), dy = in->LY / (ny - 1.0), dz = in->Lcr / (in->nz - 1.0);
+    const double dx = nx > 1 ? in->LX / (nx - 1.0) : 0.0, dy = ny > 1 ? in->LY / (ny - 1.0) : 0.0,
+                 dz = in->Lcr / (in->nz - 1.0);
     const bool phys = (in->flags & OR_PHYSICS) != 0;
     // Wavevectors: shipped kp = 2 pi ns / lp and ki = 2 pi ni / ls (Q8).
     const double kp = phys ? 2.0 * PI * n[0] / lp : 2.0 * PI * n[1] / lp;
     const double ks = 2.0 * PI * n[1] / ls;
     const double ki = phys ? 2.0 * PI * n[2] / li : 2.0 * PI * n[2] / ls;
-    const double dk = kp - ks - ki - 2.0 * PI / in->Lambda;
+    // ZGP is not quasi-phase matched: no grating term (ZGP.cuh:76)
+    const double dk = kp - ks - ki - (in->crystal == OR_ZGP ? 0.0 : 2.0 * PI / in->Lambda);
     const double kappa[3] = {2 * PI * dQ / (n[0] * lp), 2 * PI * dQ / (n[1] * ls),
                              2 * PI * dQ / (n[2] * li)};
     const double trt = (in->Lcav + in->Lcr * (n[1] - 1)) / C;
@@ -504,7 +585,9 @@ int or_setup(const OrPhys *in, OrParams *o, double *sc, double *t, double *w, do
     o->nx = nx; o->ny = ny; o->nt = nt; o->n_steps = nsteps; o->flags = in->flags;
     o->dz = (phys && in->n_steps > 0) ? in->Lcr / in->n_steps : dz;
     o->Lcr = in->Lcr; o->dx = dx; o->dy = dy;
-    for (int f = 0; f < 3; f++) { o->kappa[f] = kappa[f]; o->beta2[f] = b2[f]; o->alpha[f] = alpha[f]; }
+    for (int f = 0; f < 3; f++) {
+        o->kappa[f] = kappa[f]; o->beta2[f] = b2[f]; o->beta3[f] = b3x[f]; o->alpha[f] = alpha[f];
+    }
     o->kdiff[0] = kp; o->kdiff[1] = ks; o->kdiff[2] = ki;
     // Group-delay frame, Solver3D.cuh:163-165: pump 1/vp-1/vi, signal 0, idler 1/vi-1/vs.
     o->vinv[0] = 1 / v[0] - 1 / v[2];
@@ -516,6 +599,9 @@ int or_setup(const OrPhys *in, OrParams *o, double *sc, double *t, double *w, do
     o->free_len = in->Lcr;  // Solver3D.cuh:989
     o->total_rt = in->total_rt;
     o->rt_index = 0;
+    o->eom_beta = in->eom_beta;
+    o->eom_fpm = in->eom_fpm;
+    o->t_window = in->t_window > 0 ? in->t_window : trt;
 
     if (sc) {
         const double vals[OR_N_SCALARS] = {n[0], n[1], n[2], v[0], v[1], v[2], b2[0], b2[1], b2[2],
@@ -541,13 +627,19 @@ int or_setup(const OrPhys *in, OrParams *o, double *sc, double *t, double *w, do
         const double w02 = w0 * w0;
         const double zR = PI * n[0] * w02 / lp;
         const double eta = in->focal / zR;
-        const double Ap0 = std::sqrt(4 * P / (EPS0 * C * PI * n[0] * w02));
+        // 1-D (nx = ny = 1): EFields1D.cuh:145-148, mean intensity 2P/(pi w0^2), no focusing
+        const bool one_d = nx == 1 && ny == 1;
+        if (one_d && (in->pump_mode == OR_PUMP_FOCUSED_CW || in->pump_mode == OR_PUMP_FOCUSED_PULSED ||
+                      in->pump_mode == OR_PUMP_FOCUSED_SECH2))
+            return -3;
+        const double pk = one_d ? 2.0 : 4.0;
+        const double Ap0 = std::sqrt(pk * P / (EPS0 * C * PI * n[0] * w02));
         const cd MX(1, -eta);
         const double uX = 0.5 * nx, uY = 0.5 * ny;
         // sech^2 envelopes: |A|^2 ~ sech^2(t/ts), FWHM = 2 acosh(sqrt 2) ts; P is then the
         // window-average power, so the peak is P T / (2 ts).
         const double ts = in->FWHM / (2 * std::acosh(std::sqrt(2.0)));
-        const double Ap0s = std::sqrt(4 * (P * T / (2 * ts)) / (EPS0 * C * PI * n[0] * w02));
+        const double Ap0s = std::sqrt(pk * (P * T / (2 * ts)) / (EPS0 * C * PI * n[0] * w02));
         for (int it = 0; it < nt; it++)
             for (int y = 0; y < ny; y++)
                 for (int x = 0; x < nx; x++) {
@@ -598,7 +690,9 @@ int or_single_pass(const OrParams *p, const double *w, double *Ap, double *As, d
 
 // Round trips, Solver3D.cuh:979-1011:
 //   Ap <- Api; SSFM; if not the last round trip: free-space return of s and i by +Lcr
-//   (scale 1/(NX NY)); GDD on s and i (fixed form of :644-694); mirrors
+//   (scale 1/(NX NY)); EOM on s and i, exp(i beta sin(2 pi fpm t)) (the 1-D solver's
+//   intracavity modulator, Solver1D.cuh:63-72,467; it acts per t-plane, so it commutes
+//   with the free-space return); GDD on s and i (fixed form of :644-694); mirrors
 //   sqrt(R) e^{i phase} on the resonant s and i (Cavity3D.cuh:12-28,68-80).
 int or_round_trips(OrParams *p, const double *w, const double *Api, double *Ap, double *As,
                    double *Ai, int n_rt)
@@ -611,6 +705,18 @@ int or_round_trips(OrParams *p, const double *w, const double *Api, double *Ap, 
         r.ssfm(F);
         if (p->rt_index != p->total_rt - 1 && (p->flags & OR_DIFFRACTION))
             xyOp(p, r.cache, F, r.freeTab, 6u, 1.0 / ((double)p->nx * p->ny));
+        if (p->eom_beta != 0) {
+            const size_t plane = (size_t)p->nx * p->ny;
+            const double T = p->t_window;
+            for (int it = 0; it < p->nt; it++) {
+                const double t = -T * 0.5 + it * (T * 0.5 - (-T * 0.5)) / (p->nt - 1);
+                const cd e = cpxExp(p->eom_beta * std::sin(2 * PI * p->eom_fpm * t));
+                for (size_t v = (size_t)it * plane; v < (size_t)(it + 1) * plane; v++) {
+                    F[1][v] *= e;
+                    F[2][v] *= e;
+                }
+            }
+        }
         if (p->gdd != 0 && (p->flags & OR_DISPERSION)) {
             OrParams q = *p;
             q.flags &= ~(unsigned)OR_ASIS_Q2;

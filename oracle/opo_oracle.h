@@ -30,9 +30,10 @@ enum {
                                 absorption applied once, kp/ki from their own indices */
     OR_ASIS_Q1 = 1u << 3,    /* diffraction inverse scale 1/(NX NY NT) as shipped      */
     OR_ASIS_Q2 = 1u << 4,    /* dispersion only on row y=0, scale 1/(NX NY NT)         */
+    OR_TOD = 1u << 5,        /* not in the reference: w^3 b3 / 6 in the dispersion phase */
 };
 
-enum { OR_PPLN = 0, OR_MGOSPPLT = 1 };
+enum { OR_PPLN = 0, OR_MGOSPPLT = 1, OR_MGOPPLN = 2, OR_ZGP = 3 };
 
 enum {
     OR_PUMP_WAVEPLANE_CW = 0,
@@ -45,9 +46,10 @@ enum {
 
 /* Physical description of one run (the reference's main() parameters). */
 typedef struct {
-    int crystal;                 /* OR_PPLN / OR_MGOSPPLT                          */
+    int crystal;                 /* OR_PPLN / OR_MGOSPPLT / OR_MGOPPLN / OR_ZGP     */
     double LX, LY, Lcr, T, Lambda, lp, ls; /* um, um, um, degC, um, um, um         */
-    int nx, ny, nt, nz;          /* grid, nz = slices (dz = Lcr/(nz-1))             */
+    int nx, ny, nt, nz;          /* grid, nz = slices (dz = Lcr/(nz-1)); nx = ny = 1
+                                    (no diffraction) is the plane-wave 1-D solver     */
     double dQ;                   /* um/V; <= 0 keeps the crystal's 2 d33 / pi       */
     double alpha[3];             /* 1/um; < 0 keeps the crystal's value             */
     double Lcav, Rs, Ri;         /* um; mirror reflectivities                       */
@@ -60,6 +62,8 @@ typedef struct {
     int zloop_f32;               /* step count from the FP32 (1) or FP64 (0) loop   */
     int n_steps;                 /* > 0 overrides the loop count (physics mode)     */
     int total_rt;                /* round trips of the run (last one skips free space) */
+    unsigned pol;                /* ZGP: bit f set = wave f (p, s, i) extraordinary   */
+    double eom_beta, eom_fpm;    /* intracavity EOM (Cavity1D.cuh:75-84); beta 0: none */
 } OrPhys;
 
 /* Everything the split-step needs, derived from OrPhys. */
@@ -76,6 +80,8 @@ typedef struct {
     double Rs, Ri, detuning, gdd, free_len;
     int total_rt;
     int rt_index;       /* round trips done so far (in/out)      */
+    double beta3[3];    /* third-order dispersion (OR_TOD)       */
+    double eom_beta, eom_fpm, t_window;
 } OrParams;
 
 /* Derived scalars, in this order (the harness dump uses the same names):
@@ -86,6 +92,10 @@ typedef struct {
 int or_setup(const OrPhys *in, OrParams *out, double *scalars, double *t, double *w,
              double *Api);
 int or_zloop_steps(double Lcr, double dz, int f32);
+/* n, group velocity, GVD, TOD as the reference prints it, and the exact TOD (third
+ * derivative by central difference) of one crystal index (extraordinary selects ZGP's
+ * 'e'; ZGP has no reference TOD, both are the exact one). */
+int or_crystal_dispersion(int crystal, double T, int extraordinary, double L, double out[5]);
 void or_fft(int n, int sign, double *data);
 void or_noise(uint64_t seed, double sigma, size_t n_complex, double *out);
 int or_single_pass(const OrParams *p, const double *w, double *Ap, double *As, double *Ai);

@@ -20,8 +20,9 @@ OR_DIFFRACTION = 1 << 1
 OR_PHYSICS = 1 << 2
 OR_ASIS_Q1 = 1 << 3
 OR_ASIS_Q2 = 1 << 4
+OR_TOD = 1 << 5
 
-OR_PPLN, OR_MGOSPPLT = 0, 1
+OR_PPLN, OR_MGOSPPLT, OR_MGOPPLN, OR_ZGP = 0, 1, 2, 3
 PUMP_MODES = {
     "waveplane-cw": 0,
     "waveplane-pulsed": 1,
@@ -53,6 +54,8 @@ class OrPhys(ctypes.Structure):
         ("zloop_f32", ctypes.c_int),
         ("n_steps", ctypes.c_int),
         ("total_rt", ctypes.c_int),
+        ("pol", ctypes.c_uint),
+        ("eom_beta", ctypes.c_double), ("eom_fpm", ctypes.c_double),
     ]
 
 
@@ -70,6 +73,8 @@ class OrParams(ctypes.Structure):
         ("Rs", ctypes.c_double), ("Ri", ctypes.c_double), ("detuning", ctypes.c_double),
         ("gdd", ctypes.c_double), ("free_len", ctypes.c_double),
         ("total_rt", ctypes.c_int), ("rt_index", ctypes.c_int),
+        ("beta3", ctypes.c_double * 3),
+        ("eom_beta", ctypes.c_double), ("eom_fpm", ctypes.c_double), ("t_window", ctypes.c_double),
     ]
 
 
@@ -96,6 +101,7 @@ def lib():
         L.or_single_pass.argtypes = [ctypes.POINTER(OrParams), dp, dp, dp, dp]
         L.or_round_trips.argtypes = [ctypes.POINTER(OrParams), dp, dp, dp, dp, dp, ctypes.c_int]
         L.or_set_threads.argtypes = [ctypes.c_int]
+        L.or_crystal_dispersion.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp]
         _lib = L
     return _lib
 
@@ -112,8 +118,10 @@ def make_phys(**kw):
              alpha=(-1.0, -1.0, -1.0), Lcav=-1.0, Rs=0.98, Ri=None, gdd_gamma=0.0,
              detuning=0.0, P=1.0, FWHM=2.0, w0=50.0, focal=None, pump_mode="focused-pulsed",
              t_window=0.0, flags=OR_DISPERSION | OR_DIFFRACTION, zloop_f32=0, n_steps=0,
-             total_rt=1)
+             total_rt=1, pol="eeo", eom_beta=0.0, eom_fpm=0.0)
     d.update(kw)
+    if isinstance(d["pol"], str):
+        d["pol"] = sum(1 << f for f, ch in enumerate(d["pol"]) if ch == "e")
     if d["Ri"] is None:
         d["Ri"] = d["Rs"]
     if d["focal"] is None:
@@ -129,6 +137,15 @@ def make_phys(**kw):
         else:
             setattr(ph, k, v)
     return ph
+
+
+def crystal_dispersion(crystal, T, L, extraordinary=True):
+    """(n, vg, b2, b3 as the reference prints it, exact b3) of one crystal index."""
+    out = np.zeros(5)
+    rc = lib().or_crystal_dispersion(crystal, T, 1 if extraordinary else 0, L, _ptr(out))
+    if rc:
+        raise ValueError(f"or_crystal_dispersion: {rc}")
+    return out
 
 
 class Setup:

@@ -42,6 +42,16 @@ public:
         gdd = true;
         gamma = g;
     }
+    // Intracavity electro-optic modulator (cuOPO3D Cavity1D.cuh:75-84): after the crystal,
+    // signal and idler x exp(i beta sin(2 pi fpm t)), before GDD and the mirrors.
+    void setEOM(real_t _beta, real_t _fpm)
+    {
+        eom = true;
+        beta = _beta;
+        fpm = _fpm;
+        std::cout << "Set intracavity EOM:\n        ---> beta = " << beta << "\n        ---> fpm = " << fpm * 1e3
+                  << " GHz" << std::endl;
+    }
     void getCavityProp() const
     {
         std::cout << "Set OPO cavity:\n        ---> Cavity length         = " << Lcav * 1e-6 << " m"

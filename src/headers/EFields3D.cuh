@@ -49,6 +49,7 @@ public:
     {
         OpoConfig c = pump_set ? pump_cfg : OpoConfig{};
         c.crystal = Crystal::kind;
+        c.pol = Cr->pol_bits;
         c.LX = Cr->LX; c.LY = Cr->LY; c.Lcr = Cr->Lcr; c.T = Cr->T; c.Lambda = Cr->Lambda;
         c.lp = lp; c.ls = ls;
         c.nx = NX; c.ny = NY; c.nt = NT; c.nz = NZ;

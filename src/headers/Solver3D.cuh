@@ -87,6 +87,8 @@ private:
             c.Lcav = Cav->Lcav; c.Rs = Cav->Rs; c.Ri = Cav->Ri;
             c.gdd_gamma = Cav->gdd ? Cav->gamma : 0.0;
             c.detuning = Cav->detuning;
+            c.eom_beta = Cav->eom ? Cav->beta : 0.0;
+            c.eom_fpm = Cav->eom ? Cav->fpm : 0.0;
         } else {
             c.Lcav = -1; c.Rs = 1; c.Ri = 1; c.resonant = 0;
         }

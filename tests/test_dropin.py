@@ -25,6 +25,27 @@ def test_reference_main_compiles_unchanged(tmp_path):
     assert out.exists() and os.access(out, os.X_OK)
 
 
+@pytest.mark.skipif(not os.path.exists(REF_MAIN), reason="reference checkout not present")
+@pytest.mark.parametrize("crystal", ["ZGP", "MgOPPLN"])
+def test_reference_main_other_crystals_compile(tmp_path, crystal):
+    """The reference main with its crystal switched the way its own comments show
+    (cuOPO3D.cu:21-23: the ZGP alternative with a polarisation tuple; MgOPPLN takes
+    MgOsPPLT's constructor arguments)."""
+    src = open(REF_MAIN).read()
+    if crystal == "ZGP":
+        src = src.replace("MgOsPPLT * cr1 = new MgOsPPLT(LX, LY, Lcr, T, Lambda, lp, ls, li);", "")
+        src = src.replace("// std::tuple<char, char, char> pol", "std::tuple<char, char, char> pol")
+        src = src.replace("// ZGP * cr1 = new ZGP(", "ZGP * cr1 = new ZGP(")
+    src = src.replace("MgOsPPLT", crystal)
+    main = tmp_path / "main.cu"
+    main.write_text(src)
+    out = tmp_path / "cuOPO3D"
+    r = subprocess.run([os.path.join(ROOT, "src", "build_dropin.sh"), str(main), str(out)] + DEMO_FLAGS,
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    assert out.exists() and os.access(out, os.X_OK)
+
+
 def read_slice(path):
     re_ = np.loadtxt(path + "_r.dat")
     im = np.loadtxt(path + "_i.dat")
