@@ -386,11 +386,6 @@ struct PassTimer {
 template <typename C> C to_c(const cd &v);
 template <> float2 to_c<float2>(const cd &v) { return make_float2((float)v.real(), (float)v.imag()); }
 template <> double2 to_c<double2>(const cd &v) { return make_double2(v.real(), v.imag()); }
-template <> float4 to_c<float4>(const cd &v)
-{
-    const float hx = (float)v.real(), hy = (float)v.imag();
-    return make_float4(hx, hy, (float)(v.real() - hx), (float)(v.imag() - hy));
-}
 
 template <typename C> int upload(OpoSolver *s, std::vector<void *> &allocs, const std::vector<cd> &h, void **out)
 {

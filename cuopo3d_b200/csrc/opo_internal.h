@@ -61,11 +61,8 @@ template <typename C> struct RealOf;
 template <> struct RealOf<float2> { using type = float; };
 template <> struct RealOf<double2> { using type = double; };
 
-// Phase-table entry: complex128 for FP64 fields; for FP32 fields a float4 (hi.x, hi.y,
-// lo.x, lo.y) with hi + lo equal to the FP64 value to ~1e-15, so that a table applied
-// every z-step carries no coherent FP32 rounding bias.
+// Phase-table entry: the field's own complex type (FP64 values rounded once on upload).
 template <typename C> struct TabOf { using type = C; };
-template <> struct TabOf<float2> { using type = float4; };
 
 template <typename C> struct TPassArgs {
     using T = typename RealOf<C>::type;

@@ -32,11 +32,7 @@ template <int S, typename C> __device__ __forceinline__ C twmul(C x, C w)
 }
 
 __device__ __forceinline__ double2 tab_mul(double2 x, double2 t) { return cmul(x, t); }
-__device__ __forceinline__ float2 tab_mul(float2 x, float4 t)
-{
-    const float2 a = cmul(x, make_float2(t.x, t.y)), b = cmul(x, make_float2(t.z, t.w));
-    return make_float2(a.x + b.x, a.y + b.y);
-}
+__device__ __forceinline__ float2 tab_mul(float2 x, float2 t) { return cmul(x, t); }
 
 __device__ __forceinline__ unsigned tile_base(const TileGeom &g, unsigned tile)
 {

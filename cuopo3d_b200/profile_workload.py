@@ -2,7 +2,7 @@
 round trip per step) with a pinned kernel configuration, so that an ncu launch list has
 a fixed launch order: 4 field-conversion kernels (fields uploaded from FP64 host
 arrays), then per round trip n t-passes, n x- and y-passes, the closing t-pass and the
-free-space x'/y' passes (3n + 3 launches).
+free-space x'/y' passes (3n + 3 launches; with --plane K the x and y passes are one plane pass: 2n + 2).
 
     python -m cuopo3d_b200.profile_workload --precision fp32 --round-trips 1
 """
@@ -24,6 +24,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--precision", default="fp32", choices=("fp32", "fp64"))
     ap.add_argument("--round-trips", type=int, default=1)
+    ap.add_argument("--plane", type=int, default=0,
+                    help="fused (x, y) plane pass cluster size; 0 runs the separate x and y passes")
     a = ap.parse_args()
     prec = co.FP64 if a.precision == "fp64" else co.FP32
     cfg = co.make_config(nx=128, ny=128, nt=256, nz=100, LX=800.0, LY=800.0, Lcr=20000.0, t_window=40.0,
@@ -33,6 +35,7 @@ def main():
     _, w = co.time_freq(cfg.nt, params.t_window)
     sim = co.Simulation(params, w)
     sim.set_tuning(TUNED[a.precision])
+    sim.set_plane_pass(a.plane)
     api = co.pump_field(cfg)
     s0 = co.noise(1, 1e-6 * float(np.max(np.abs(api))), api.size).reshape(api.shape)
     for which, arr in ((co.FIELD_API, api), (co.FIELD_AP, api), (co.FIELD_AS, s0),
