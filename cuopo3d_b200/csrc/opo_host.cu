@@ -502,11 +502,13 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
         g.nlines = P; g.ntiles = (nx / P) * ny;
         g.lsl = 1; g.lsj = P; g.region = (unsigned)(nt * P);
         g.tdiv = make_fastdiv(nx / P); g.tmulA = P; g.tmulB = nx; g.gs_j = nxy; g.gs_l = 1;
+        g.pairs = (P % 2 == 0 && nx % 2 == 0) ? 1 : 0;
     } else if (kind == kY) {
         const int Py = largest_divisor_leq(nx, (int)(te / ny));
         g.nlines = Py; g.ntiles = (nx / Py) * nt;
         g.lsl = 1; g.lsj = Py; g.region = (unsigned)(ny * Py);
         g.tdiv = make_fastdiv(nx / Py); g.tmulA = Py; g.tmulB = nxy; g.gs_j = nx; g.gs_l = 1;
+        g.pairs = (Py % 2 == 0 && nx % 2 == 0) ? 1 : 0;
     } else {
         // x tiles: whole rows, stored row by row with an odd row stride nx + 1 so that
         // the line-parallel middle stages (consecutive threads on consecutive rows) and
@@ -517,6 +519,7 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
         g.tdiv = make_fastdiv(1); g.tmulA = 0; g.tmulB = (unsigned)rows * nx; g.gs_j = 1; g.gs_l = nx;
     }
     g.nl = make_fastdiv((unsigned)g.nlines);
+    g.rowlen = make_fastdiv((unsigned)nx);
     g.region = (g.region + 1u) & ~1u;  // keeps every field region 16-byte aligned
     pc.smem = 3 * (size_t)g.region * sizeof(C);
     if (pc.smem > 227 * 1024) return fail(s, OPO_ERR_INVALID, "tile does not fit in shared memory");

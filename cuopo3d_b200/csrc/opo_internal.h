@@ -52,9 +52,11 @@ struct TileGeom {
     int ntiles;
     unsigned lsl, lsj, region;
     FastDiv tdiv;
-    FastDiv nl;  // nlines
+    FastDiv nl;      // nlines
+    FastDiv rowlen;  // x tiles: line length nx (row-major staging)
     unsigned tmulA, tmulB;
     unsigned gs_j, gs_l;
+    int pairs;       // t / y tiles: line pairs start 16-byte aligned (FP32 staging by 16 B)
 };
 
 template <typename C> struct RealOf;

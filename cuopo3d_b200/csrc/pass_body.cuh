@@ -40,6 +40,58 @@ __device__ __forceinline__ unsigned tile_base(const TileGeom &g, unsigned tile)
     return (tile - hi * g.tdiv.d) * g.tmulA + hi * g.tmulB;
 }
 
+// ---------------------------------------------------------------------------------
+// Tile staging with cp.async: every thread issues its share of the whole tile (all
+// fields) as asynchronous global -> shared copies, so a tile costs one memory latency
+// however many fields and items it has, and no registers hold the data in flight.
+// Completion is the hardware wait cp.async.wait_all (no polling loop).
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+template <int BYTES> __device__ __forceinline__ void cp_async(void *dst, const void *src)
+{
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Copy the raw lines of tile `tile` of the fields in mask (field f from src[f]) into their
+// shared-memory regions: t / y tiles element e = j nlines + l (lines contiguous in global
+// memory, two at a time when g.pairs), x tiles element e = l nx + j (rows contiguous),
+// placed at l lsl + j.
+template <typename C, int THREADS, bool ROWMAJOR>
+__device__ __forceinline__ void stage_tile(const TileGeom &g, unsigned n, unsigned tile, const C *const *src,
+                                           unsigned mask, C *sm)
+{
+    const unsigned base = tile_base(g, tile);
+    const unsigned count = n * (unsigned)g.nlines;
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+        if (!(mask & (1u << f))) continue;
+        const C *gsrc = src[f] + base;
+        C *dst = sm + (size_t)f * g.region;
+        if (ROWMAJOR) {
+            for (unsigned e = threadIdx.x; e < count; e += THREADS) {
+                const unsigned l = fdiv(g.rowlen, e), j = e - l * n;
+                cp_async<sizeof(C)>(dst + l * g.lsl + j, gsrc + e);
+            }
+        } else if (sizeof(C) == 8 && g.pairs) {
+            for (unsigned e = 2 * threadIdx.x; e < count; e += 2 * THREADS) {
+                const unsigned j = fdiv(g.nl, e), l = e - j * g.nlines;
+                cp_async<16>(dst + l + j * g.lsj, gsrc + j * g.gs_j + l);
+            }
+        } else {
+            for (unsigned e = threadIdx.x; e < count; e += THREADS) {
+                const unsigned j = fdiv(g.nl, e), l = e - j * g.nlines;
+                cp_async<sizeof(C)>(dst + l + j * g.lsj, gsrc + j * g.gs_j + l);
+            }
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+}
+
 // Index of the f-th field (in p, s, i order) selected by mask.
 __device__ __forceinline__ int field_id(unsigned mask, int f)
 {
@@ -302,7 +354,7 @@ template <typename C> __device__ __forceinline__ unsigned tpass_load_mask(const 
 // n_rk4 half steps to each voxel, then the first forward stage of every transformed
 // field into its shared-memory region (untransformed fields go back to global).
 
-template <typename C, int R1, int THREADS, int RMAX>
+template <typename C, int R1, int THREADS, int RMAX, bool STAGED = false>
 __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile, C *sm)
 {
     const AxisPlan &p = a.plan;
@@ -324,7 +376,7 @@ __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile,
             const C *gsrc = f == 0 ? a.psrc : a.f[f];
 #pragma unroll
             for (int m = 0; m < R1; m++)
-                x[f][m] = gsrc[gb + m * gstep];
+                x[f][m] = STAGED ? sm[f * g.region + l + (b + m * q) * lsj] : gsrc[gb + m * gstep];
         }
         for (int h = 0; h < a.n_rk4; h++) {
 #pragma unroll
@@ -366,7 +418,7 @@ __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile,
 // consecutive butterflies of a line (x axis, where lines are rows and the transform
 // index is the contiguous one); otherwise consecutive threads take consecutive lines.
 
-template <typename C, int R1, bool BFAST, int THREADS, int RMAX>
+template <typename C, int R1, bool BFAST, int THREADS, int RMAX, bool STAGED = false>
 __device__ __forceinline__ void axis_tile(const AxisArgs<C> &a, unsigned tile, C *sm)
 {
     const AxisPlan &p = a.plan;
@@ -395,7 +447,7 @@ __device__ __forceinline__ void axis_tile(const AxisArgs<C> &a, unsigned tile, C
             C *s = sf + l * g.lsl + b * g.lsj;
             C x[R1];
 #pragma unroll
-            for (int m = 0; m < R1; m++) x[m] = srcf[l * g.gs_l + (b + m * q) * g.gs_j];
+            for (int m = 0; m < R1; m++) x[m] = STAGED ? s[m * q * g.lsj] : srcf[l * g.gs_l + (b + m * q) * g.gs_j];
             dft<R1, -1>(x);
 #pragma unroll
             for (int k = 1; k < R1; k++) x[k] = twmul<-1>(x[k], __ldg(a.tw + (k - 1) * q + b));

@@ -9,15 +9,22 @@ namespace opo {
 
 // Single-instance kernels: the grid walks the tiles of one solver.  Several CTAs per SM
 // (each a tile of 3 fields in shared memory) overlap one another's global loads, the
-// shared-memory stages and the stores.
+// shared-memory stages and the stores.  The t-pass stages its whole tile with cp.async
+// first (one memory latency per tile for its 12 loads per item); the axis passes, with
+// fewer values per item, load straight into registers in their first stage, which
+// measured faster for them.
 
 template <typename C, int R1, int THREADS, int RMAX>
 __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 4 : 1) tpass_kernel(TPassArgs<C> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *sm = reinterpret_cast<C *>(smem_raw);
-    for (unsigned tile = blockIdx.x; tile < (unsigned)a.g.ntiles; tile += gridDim.x)
-        tpass_tile<C, R1, THREADS, RMAX>(a, tile, sm);
+    const C *src[3] = {a.psrc, a.f[1], a.f[2]};
+    const unsigned lmask = tpass_load_mask(a);
+    for (unsigned tile = blockIdx.x; tile < (unsigned)a.g.ntiles; tile += gridDim.x) {
+        stage_tile<C, THREADS, false>(a.g, (unsigned)a.plan.n, tile, src, lmask, sm);
+        tpass_tile<C, R1, THREADS, RMAX, true>(a, tile, sm);
+    }
 }
 
 template <typename C, int R1, bool BFAST, int THREADS, int RMAX>
