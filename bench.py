@@ -165,17 +165,20 @@ def upload(co, sim, api, s0):
         sim.set_field(which, arr)
 
 
-def time_device(sim, steps, world):
-    """K round trips between events on the solver's stream; max over ranks (ms)."""
+def time_device(sim, steps, world, tag):
+    """K round trips between events on the solver's stream; max over ranks (ms).  The
+    region is an NVTX range named timed_<tag>, so a profiler can select its launches."""
     import torch
     stream = torch.cuda.ExternalStream(sim.stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier_sync(world)
     sim.synchronize()
+    torch.cuda.nvtx.range_push(f"timed_{tag}")
     e0.record(stream)
     sim.run_round_trips(steps)
     e1.record(stream)
     sim.synchronize()
+    torch.cuda.nvtx.range_pop()
     barrier_sync(world)
     return max_over_ranks(e0.elapsed_time(e1), world)
 
@@ -195,7 +198,7 @@ def run_ours(args):
         sim.synchronize()
         l0 = sim.kernel_launches
         with ClockSampler(local) as clk:
-            ms = time_device(sim, args.steps, world)
+            ms = time_device(sim, args.steps, world, tag)
         launches = sim.kernel_launches - l0
         vsteps = float(V) * nsteps * args.steps
         total_vsteps = sum_over_ranks(vsteps, world)
@@ -270,7 +273,7 @@ def run_ours(args):
             "tuning_fp64": main["tuning"],
             "fp32": {"value": out["fp32"]["value"], "ms_per_step": out["fp32"]["ms_per_step"],
                      "passes": out["fp32"]["passes"], "e2e": out["fp32"]["e2e"],
-                     "clocks": out["fp32"]["clocks"]},
+                     "clocks": out["fp32"]["clocks"], "tuning": out["fp32"]["tuning"]},
         }
         if not args.no_forms:
             tun = out["fp32"]["tuning"]

@@ -13,7 +13,7 @@ import numpy as np
 import cuopo3d_b200 as co
 
 TUNED = {
-    "fp32": {"t": dict(threads=128, tile=2048, r1=4), "x": dict(threads=128, tile=2048, r1=16),
+    "fp32": {"t": dict(threads=128, tile=2048, r1=4), "x": dict(threads=128, tile=2048, r1=8),
              "y": dict(threads=128, tile=2048, r1=16)},
     "fp64": {"t": dict(threads=128, tile=1024, r1=4), "x": dict(threads=128, tile=1024, r1=8),
              "y": dict(threads=128, tile=1024, r1=8)},
