@@ -494,7 +494,9 @@ int opo_batch_create(int precision, int capacity, size_t hbm_budget, const int t
     const bool fp64 = precision == OPO_FP64;
     for (int k = 0; k < 3; k++) {
         if (tuning) {
-            b->v[k] = opo::PassVariant{tuning[3 * k], tuning[3 * k + 2]};
+            // the batched kernels have no warp-specialised form: a warp-specialised CTA
+            // size (160 / 288) runs as its consumer size (128 / 256)
+            b->v[k] = opo::PassVariant{opo::consumer_threads(opo::PassVariant{tuning[3 * k], 0}), tuning[3 * k + 2]};
             b->te[k] = (size_t)tuning[3 * k + 1];
         } else {
             b->v[k] = opo::PassVariant{128, k == 0 ? 4 : 8};

@@ -6,6 +6,8 @@
 #include "opo_internal.h"
 #include "solver_internal.h"
 
+#include <cudaTypedefs.h>
+
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -281,6 +283,10 @@ struct PassCfg {
     void *tw = nullptr;
     void *tab[2][3] = {};
     void *eom = nullptr;  // t-pass: EOM phase per time sample (natural order), or null
+    // warp-specialised variant: ring arguments and the tensor maps of the fields
+    // (t-pass: Api, Ap, As, Ai; y-pass: Ap, As, Ai)
+    opo::WsArgs wsa{};
+    CUtensorMap maps[4];
     std::vector<void *> allocs;
 };
 
@@ -314,6 +320,7 @@ struct OpoSolver {
     void *field[4] = {};  // Api, Ap, As, Ai
     PassCfg pass[3];
     PlaneCfg plane;
+    int *err_dev = nullptr;  // error word of the warp-specialised passes
     std::vector<double> w;
     double *partials = nullptr, *sums_dev = nullptr;
     int sum_blocks = 0;
@@ -351,6 +358,19 @@ int cuda_fail(OpoSolver *s, cudaError_t e, const char *what)
         cudaError_t e_ = (call);                                \
         if (e_ != cudaSuccess) return cuda_fail((s), e_, what); \
     } while (0)
+
+// After a synchronisation with the solver's stream: a warp-specialised pass that gave up
+// on a bounded wait left a code in the error word (cleared here).
+int check_pass_error(OpoSolver *s)
+{
+    if (!s->err_dev) return OPO_OK;
+    int code = 0;
+    OPO_CU(s, cudaMemcpy(&code, s->err_dev, sizeof(int), cudaMemcpyDeviceToHost), "error word");
+    if (!code) return OPO_OK;
+    cudaMemset(s->err_dev, 0, sizeof(int));
+    return fail(s, OPO_ERR_CUDA, "a warp-specialised pass stopped after a pipeline wait timed out (code " +
+                                     std::to_string(code) + ")");
+}
 
 cudaEvent_t take_event(OpoSolver *s)
 {
@@ -433,6 +453,40 @@ void drop_graphs(OpoSolver *s)
         }
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            (void)cudaGetLastError();
+    });
+    return fn;
+}
+
+// Tensor map of one field viewed as a 3-D tensor (nx * m, ny, nt) of 8-byte elements,
+// m = complex bytes / 8, with box (box0, box1, box2).
+bool encode_field_map(CUtensorMap *map, void *field, int nx, int ny, int nt, size_t esz, unsigned box0,
+                      unsigned box1, unsigned box2)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)nx * (esz / 8), (cuuint64_t)ny, (cuuint64_t)nt};
+    const cuuint64_t strides[2] = {(cuuint64_t)nx * esz, (cuuint64_t)nx * ny * esz};
+    const cuuint32_t box[3] = {box0, box1, box2};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, field, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Diffraction factor tables of the x axis (xa) or the y axis in the digit-reversed order
 // of plan pl: the propagator exp(sign L 2 pi^2 / k (fx^2 + fy^2)) of Solver3D.cuh:282-323
 // factorised as (x factor)(y factor); fx = centred(i) / (dx nx).  crys[f] is the crystal
@@ -492,7 +546,7 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     std::vector<cd> tw;
     int r1 = v.r1;
     if (fp64 && kind == kT && r1 > 8) r1 = 8;  // 3 fields x r1 complex128 live in registers
-    while (r1 >= 4 && !build_plan(n, r1, opo::max_radix(fp64, v.threads), pc.plan, tw)) r1 /= 2;
+    while (r1 >= 4 && !build_plan(n, r1, opo::max_radix(fp64, opo::consumer_threads(v)), pc.plan, tw)) r1 /= 2;
     if (r1 < 4) return fail(s, OPO_ERR_INVALID, "grid sizes must be 2^a 3^b and >= 8");
     pc.v.r1 = r1;
     const unsigned nxy = (unsigned)nx * ny;
@@ -521,8 +575,51 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     g.nl = make_fastdiv((unsigned)g.nlines);
     g.rowlen = make_fastdiv((unsigned)nx);
     g.region = (g.region + 1u) & ~1u;  // keeps every field region 16-byte aligned
+    const bool ws = opo::is_ws(v);
+    if (ws) {
+        // tensor / bulk copies land on 128-byte boundaries
+        const unsigned per128 = (unsigned)(128 / sizeof(C));
+        g.region = (g.region + per128 - 1) / per128 * per128;
+    }
     pc.smem = 3 * (size_t)g.region * sizeof(C);
     if (pc.smem > 227 * 1024) return fail(s, OPO_ERR_INVALID, "tile does not fit in shared memory");
+    if (ws) {
+        opo::WsArgs &w = pc.wsa;
+        const size_t es = sizeof(C);
+        w = opo::WsArgs{};
+        w.nstages = 2;
+        w.stage_bytes = (unsigned)pc.smem;
+        w.inner_mult = (unsigned)(es / 8);
+        if (kind == kX) {
+            if (((size_t)(nx + 1) * es) % 16 != 0)
+                return fail(s, OPO_ERR_INVALID, "warp-specialised x-pass needs 16-byte row strides (FP64)");
+            w.mode = opo::kWsRows;
+            w.row_bytes = (unsigned)(nx * es);
+            w.field_bytes = (unsigned)(g.nlines * nx * es);
+        } else {
+            const unsigned px = (unsigned)g.nlines, lines = (unsigned)n;
+            if ((px * es) % 16 != 0 || ((size_t)nx * es) % 16 != 0)
+                return fail(s, OPO_ERR_INVALID, "warp-specialised pass needs 16-byte tile rows");
+            unsigned bl = lines < 256 ? lines : 256;
+            while (lines % bl) bl--;
+            if (bl < lines && ((size_t)bl * px * es) % 128 != 0)
+                return fail(s, OPO_ERR_INVALID, "warp-specialised pass: box rows would start off 128-byte boundaries");
+            w.mode = opo::kWsTensor;
+            w.px = px;
+            w.line_dim = kind == kT ? 2 : 1;
+            w.lines = lines;
+            w.box_lines = bl;
+            w.field_bytes = (unsigned)(lines * px * es);
+            const unsigned b0 = px * w.inner_mult;
+            const int first = kind == kT ? 0 : 1;  // t-pass maps Api, Ap, As, Ai; y-pass Ap, As, Ai
+            for (int k = first; k < 4; k++)
+                if (!encode_field_map(&pc.maps[k - first], s->field[k], nx, ny, nt, es, b0, kind == kT ? 1 : bl,
+                                      kind == kT ? bl : 1))
+                    return fail(s, OPO_ERR_INVALID, "tensor map encoding failed");
+        }
+        pc.smem = opo::kWsHeaderBytes + w.nstages * (size_t)w.stage_bytes;
+        if (pc.smem > 227 * 1024) return fail(s, OPO_ERR_INVALID, "stage ring does not fit in shared memory");
+    }
 
     int rc;
     if ((rc = upload<C>(s, pc.allocs, tw, &pc.tw))) { free_pass(pc); return rc; }
@@ -577,6 +674,17 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
             }
     }
     pc.grid = g.ntiles;
+    if (ws) {
+        // persistent: every resident CTA, at most one per tile
+        int nsm = 0, per = 0;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->dev);
+        per = opo::ws_occupancy<C>(kind == kT, opo::PassVariant{v.threads - 32, pc.v.r1}, kind == kX, pc.smem);
+        if (per < 1 || nsm < 1) {
+            free_pass(pc);
+            return fail(s, OPO_ERR_INVALID, "warp-specialised pass cannot be resident");
+        }
+        pc.grid = std::min(g.ntiles, per * nsm);
+    }
     drop_graphs(s);
     free_pass(s->pass[kind]);
     s->pass[kind] = pc;
@@ -748,7 +856,16 @@ int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, int wh
     const PassCfg &pc = s->pass[kT];
     const opo::TPassArgs<C> a = opo::make_tpass_args<C>(s, reset_pump, n_rk4, zh, which_tab, tmask);
     PassTimer timer(s, 0);
-    OPO_CU(s, opo::launch_tpass<C>(a, pc.v, pc.grid, pc.smem, s->stream), "t-pass launch");
+    if (opo::is_ws(pc.v)) {
+        opo::WsArgs w = pc.wsa;
+        w.err = s->err_dev;
+        const CUtensorMap maps[3] = {pc.maps[reset_pump ? 0 : 1], pc.maps[2], pc.maps[3]};
+        OPO_CU(s, opo::launch_tpass_ws<C>(a, w, maps, opo::PassVariant{pc.v.threads - 32, pc.v.r1}, pc.grid, pc.smem,
+                                          s->stream),
+               "t-pass launch");
+    } else {
+        OPO_CU(s, opo::launch_tpass<C>(a, pc.v, pc.grid, pc.smem, s->stream), "t-pass launch");
+    }
     s->launches++;
     return OPO_OK;
 }
@@ -758,7 +875,15 @@ template <typename C> int enqueue_axis(OpoSolver *s, int kind, int which_tab, un
     const PassCfg &pc = s->pass[kind];
     const opo::AxisArgs<C> a = opo::make_axis_args<C>(s, kind, which_tab, mask);
     PassTimer timer(s, kind);
-    OPO_CU(s, opo::launch_axis<C>(a, pc.v, kind == kX, pc.grid, pc.smem, s->stream), "axis-pass launch");
+    if (opo::is_ws(pc.v)) {
+        opo::WsArgs w = pc.wsa;
+        w.err = s->err_dev;
+        OPO_CU(s, opo::launch_axis_ws<C>(a, w, pc.maps, opo::PassVariant{pc.v.threads - 32, pc.v.r1}, kind == kX,
+                                         pc.grid, pc.smem, s->stream),
+               "axis-pass launch");
+    } else {
+        OPO_CU(s, opo::launch_axis<C>(a, pc.v, kind == kX, pc.grid, pc.smem, s->stream), "axis-pass launch");
+    }
     s->launches++;
     return OPO_OK;
 }
@@ -915,6 +1040,7 @@ template <typename C> int field_sums(OpoSolver *s, double out[3])
     s->launches += 2;
     OPO_CU(s, cudaMemcpyAsync(out, s->sums_dev, 3 * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "sums copy");
     OPO_CU(s, cudaStreamSynchronize(s->stream), "sums sync");
+    if (int rc = check_pass_error(s)) return rc;
     for (int k = 0; k < 3; k++)
         if (!std::isfinite(out[k])) return fail(s, OPO_ERR_NONFINITE, "a field is not finite");
     return OPO_OK;
@@ -1005,7 +1131,7 @@ template <typename C> int autotune(OpoSolver *s)
     }
     TuneEntry best{key, {}, {}, {0, 256, 8}};
     const size_t tes[3] = {fp64 ? 512u : 1024u, fp64 ? 1024u : 2048u, fp64 ? 2048u : 4096u};
-    const int threads[2] = {128, 256};
+    const int threads[4] = {128, 256, 160, 288};  // 160 / 288: warp-specialised
     const int r1s[3] = {4, 8, 16};
     const long long launches0 = s->launches;
     for (int kind = 0; kind < 3; kind++) {
@@ -1284,8 +1410,14 @@ static int create_impl(const OpoParams *p, const double *w, const opo::PassVaria
         if (rc) break;
         // The attribute is per kernel function and shared by every solver of the process:
         // always allow the full 227 KB so no solver lowers it under another.
+        if ((e = cudaMalloc((void **)&s->err_dev, sizeof(int))) != cudaSuccess ||
+            (e = cudaMemset(s->err_dev, 0, sizeof(int))) != cudaSuccess) {
+            rc = cuda_fail(s, e, "cudaMalloc(error word)");
+            break;
+        }
         if ((e = opo::configure_kernels(227 * 1024)) != cudaSuccess ||
-            (e = opo::configure_plane_kernels(227 * 1024)) != cudaSuccess) {
+            (e = opo::configure_plane_kernels(227 * 1024)) != cudaSuccess ||
+            (e = opo::configure_ws_kernels(227 * 1024)) != cudaSuccess) {
             rc = cuda_fail(s, e, "configure kernels");
             break;
         }
@@ -1342,6 +1474,7 @@ void opo_destroy(OpoSolver *s)
         if (f) cudaFree(f);
     if (s->partials) cudaFree(s->partials);
     if (s->staging) cudaFree(s->staging);
+    if (s->err_dev) cudaFree(s->err_dev);
     for (auto &pc : s->pass) free_pass(pc);
     free_plane(s->plane);
     if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
@@ -1398,7 +1531,10 @@ int opo_get_field(OpoSolver *s, int which, void *dst, int where, int prec)
         s->launches++;
         OPO_CU(s, cudaMemcpyAsync(dst, s->staging, dbytes, kind, s->stream), "get_field staging copy");
     }
-    if (where == OPO_MEM_HOST) OPO_CU(s, cudaStreamSynchronize(s->stream), "get_field sync");
+    if (where == OPO_MEM_HOST) {
+        OPO_CU(s, cudaStreamSynchronize(s->stream), "get_field sync");
+        return check_pass_error(s);
+    }
     return OPO_OK;
 }
 
@@ -1424,7 +1560,7 @@ int opo_synchronize(OpoSolver *s)
 {
     if (!s) return OPO_ERR_INVALID;
     OPO_CU(s, cudaStreamSynchronize(s->stream), "synchronize");
-    return OPO_OK;
+    return check_pass_error(s);
 }
 
 int opo_set_pass_timing(OpoSolver *s, int enable)

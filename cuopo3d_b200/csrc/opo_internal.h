@@ -2,6 +2,7 @@
 // (ssfm_kernels.cu).  Not part of the C-ABI.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stddef.h>
 
@@ -116,19 +117,44 @@ template <typename C> struct PlaneArgs {
     unsigned regionA;   // elements of the slab region (the column region follows it)
 };
 
+// Warp-specialised passes (ws_pass.cu): a producer warp streams tiles into a ring of
+// shared-memory stages with TMA (tensor copies of t / y tiles over the field viewed as a
+// 3-D tensor (nx, ny, nt) of 8-byte elements, or one bulk copy per x-tile row); the
+// consumer warps run the tile bodies.  Shared memory: kWsHeaderBytes of mbarriers and a
+// flag, then nstages stages of stage_bytes.
+constexpr unsigned kWsMaxStages = 4;
+constexpr unsigned kWsHeaderBytes = 128;
+enum { kWsTensor = 0, kWsRows = 1 };
+struct WsArgs {
+    int *err;               // error word in global memory (0: no error)
+    unsigned nstages;       // ring depth (<= kWsMaxStages)
+    unsigned stage_bytes;   // one stage: the three field regions (128-byte multiple)
+    unsigned field_bytes;   // bytes one field's copies of a tile deliver
+    int mode;               // kWsTensor / kWsRows
+    // tensor mode: tile -> (tile % tdiv, tile / tdiv) = (x block, row y or plane t); the box
+    // covers px pixels (inner, px * inner_mult elements) and box_lines lines along
+    // line_dim (2: t for the t-pass, 1: y for the y-pass); lines / box_lines boxes per field
+    unsigned px, inner_mult, line_dim, lines, box_lines;
+    unsigned row_bytes;     // rows mode: bytes per row copy
+};
+
 // Kernel variant of one pass: CTA size and first-stage radix; the largest radix any
 // stage may use follows from the precision and CTA size (max_radix()).
 struct PassVariant {
-    int threads;  // 128 or 256
+    int threads;  // 128 or 256; 160 or 288: warp-specialised (128 / 256 consumers + a producer warp)
     int r1;       // 4, 8 or 16
 };
 
+inline bool is_ws(PassVariant v) { return v.threads == 160 || v.threads == 288; }
+inline int consumer_threads(PassVariant v) { return is_ws(v) ? v.threads - 32 : v.threads; }
 inline int max_radix(bool fp64, int threads) { return (fp64 && threads == 128) ? 8 : 16; }
+bool ws_variant_compiled(bool fp64, bool tpass, PassVariant consumers);
 
 // Whether (threads, r1) is one of the compiled variants (OPO_T_VARIANTS / OPO_A_VARIANTS
 // in ssfm_kernels.cu) for the t-pass (tpass = true) or the axis passes.
 inline bool variant_compiled(bool fp64, bool tpass, PassVariant v)
 {
+    if (is_ws(v)) return ws_variant_compiled(fp64, tpass, PassVariant{v.threads - 32, v.r1});
     if (v.threads != 128 && v.threads != 256) return false;
     if (v.r1 != 4 && v.r1 != 8 && v.r1 != 16) return false;
     if (!fp64) return true;
@@ -148,6 +174,16 @@ template <typename C> cudaError_t launch_sums(const C *f0, const C *f1, const C 
 cudaError_t launch_convert_d2f(const double2 *src, float2 *dst, size_t n, cudaStream_t st);
 cudaError_t launch_convert_f2d(const float2 *src, double2 *dst, size_t n, cudaStream_t st);
 cudaError_t configure_kernels(size_t max_smem);
+// Warp-specialised launchers (ws_pass.cu); v.threads = consumer threads (128 / 256).
+// maps: tensor maps of the three fields the pass loads (t-pass: pump source, signal, idler).
+cudaError_t configure_ws_kernels(size_t max_smem);
+template <typename C> int ws_occupancy(bool tpass, PassVariant v, bool bfast, size_t smem);
+template <typename C>
+cudaError_t launch_tpass_ws(const TPassArgs<C> &a, const WsArgs &w, const CUtensorMap *maps, PassVariant v, int grid,
+                            size_t smem, cudaStream_t st);
+template <typename C>
+cudaError_t launch_axis_ws(const AxisArgs<C> &a, const WsArgs &w, const CUtensorMap *maps, PassVariant v, bool bfast,
+                           int grid, size_t smem, cudaStream_t st);
 
 // Plane pass (plane_pass.cu).  Compiled CTA sizes: 256 and 512; the largest radix is
 // plane_max_radix().  grid = planes x K CTAs in clusters of K.

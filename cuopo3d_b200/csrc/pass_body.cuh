@@ -92,6 +92,17 @@ __device__ __forceinline__ void stage_tile(const TileGeom &g, unsigned n, unsign
     __syncthreads();
 }
 
+// CTA-wide barrier of a tile body: BAR = 0 is __syncthreads(); BAR > 0 is named
+// barrier 1 over the first BAR threads (the consumer warps of a warp-specialised CTA,
+// whose producer warp never joins it).
+template <int BAR> __device__ __forceinline__ void tile_sync()
+{
+    if constexpr (BAR == 0)
+        __syncthreads();
+    else
+        asm volatile("bar.sync 1, %0;\n" ::"n"(BAR) : "memory");
+}
+
 // Index of the f-th field (in p, s, i order) selected by mask.
 __device__ __forceinline__ int field_id(unsigned mask, int f)
 {
@@ -199,21 +210,21 @@ __device__ void fused_dispatch(int R, C *sm, const TileGeom &g, int n, const typ
 
 // Stages 1 .. ns-1 forward, fused middle, inverse back to stage 1 (stage 0 is fused
 // with the global load / store by the caller).
-template <typename C, int SF, int THREADS, int RMAX>
+template <typename C, int SF, int THREADS, int RMAX, int BAR = 0>
 __device__ __forceinline__ void middle_stages(C *sm, const TileGeom &g, const AxisPlan &p, const C *tw,
                               const typename TabOf<C>::type *const *tab, unsigned mask)
 {
     for (int s = 1; s < p.ns - 1; s++) {
         smem_stage_dispatch<C, SF, false, THREADS, RMAX>(p.radix[s], sm, g, p.n, p.len[s], p.q[s],
                                                          tw + p.twoff[s], mask);
-        __syncthreads();
+        tile_sync<BAR>();
     }
     fused_dispatch<C, SF, THREADS, RMAX>(p.radix[p.ns - 1], sm, g, p.n, tab, mask);
-    __syncthreads();
+    tile_sync<BAR>();
     for (int s = p.ns - 2; s >= 1; s--) {
         smem_stage_dispatch<C, -SF, true, THREADS, RMAX>(p.radix[s], sm, g, p.n, p.len[s], p.q[s],
                                                          tw + p.twoff[s], mask);
-        __syncthreads();
+        tile_sync<BAR>();
     }
 }
 
@@ -354,7 +365,7 @@ template <typename C> __device__ __forceinline__ unsigned tpass_load_mask(const 
 // n_rk4 half steps to each voxel, then the first forward stage of every transformed
 // field into its shared-memory region (untransformed fields go back to global).
 
-template <typename C, int R1, int THREADS, int RMAX, bool STAGED = false>
+template <typename C, int R1, int THREADS, int RMAX, bool STAGED = false, int BAR = 0>
 __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile, C *sm)
 {
     const AxisPlan &p = a.plan;
@@ -405,11 +416,11 @@ __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile,
             }
         }
     }
-    __syncthreads();
+    tile_sync<BAR>();
     if (!tmask) return;
-    middle_stages<C, +1, THREADS, RMAX>(sm, g, p, a.tw, a.tab, tmask);
+    middle_stages<C, +1, THREADS, RMAX, BAR>(sm, g, p, a.tw, a.tab, tmask);
     final_stage<C, R1, -1, false, THREADS>(sm, g, n, base, a.f, a.tw, p.q[0], tmask);
-    __syncthreads();
+    tile_sync<BAR>();
 }
 
 // ---------------------------------------------------------------------------------
@@ -418,7 +429,7 @@ __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile,
 // consecutive butterflies of a line (x axis, where lines are rows and the transform
 // index is the contiguous one); otherwise consecutive threads take consecutive lines.
 
-template <typename C, int R1, bool BFAST, int THREADS, int RMAX, bool STAGED = false>
+template <typename C, int R1, bool BFAST, int THREADS, int RMAX, bool STAGED = false, int BAR = 0>
 __device__ __forceinline__ void axis_tile(const AxisArgs<C> &a, unsigned tile, C *sm)
 {
     const AxisPlan &p = a.plan;
@@ -427,7 +438,7 @@ __device__ __forceinline__ void axis_tile(const AxisArgs<C> &a, unsigned tile, C
     const int nf = __popc(a.tmask);
     const unsigned items = q * NL;
     if (nf == 0) {
-        __syncthreads();
+        tile_sync<BAR>();
         return;
     }
     const unsigned base = tile_base(g, tile);
@@ -455,10 +466,10 @@ __device__ __forceinline__ void axis_tile(const AxisArgs<C> &a, unsigned tile, C
             for (int k = 0; k < R1; k++) s[k * q * g.lsj] = x[k];
         }
     }
-    __syncthreads();
-    middle_stages<C, -1, THREADS, RMAX>(sm, g, p, a.tw, a.tab, a.tmask);
+    tile_sync<BAR>();
+    middle_stages<C, -1, THREADS, RMAX, BAR>(sm, g, p, a.tw, a.tab, a.tmask);
     final_stage<C, R1, +1, BFAST, THREADS>(sm, g, n, base, a.f, a.tw, p.q[0], a.tmask);
-    __syncthreads();
+    tile_sync<BAR>();
 }
 
 }  // namespace opo

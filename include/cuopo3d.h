@@ -223,7 +223,11 @@ int opo_autotune(OpoSolver *s);
 int opo_set_tuning(OpoSolver *s, const int tuning[9]);
 
 /* Chosen configuration: for the t-, x- and y-pass in turn, {CTA threads, tile elements
- * per field, first-stage radix}.  No counterpart in the reference. */
+ * per field, first-stage radix}.  CTA threads 160 or 288 select the warp-specialised
+ * kernels: 128 or 256 consumer threads plus one producer warp that streams the tiles
+ * into a two-stage shared-memory ring with TMA (t- and y-passes in both precisions,
+ * x-pass in FP64); batches run such a setting as its consumer CTA size.  No counterpart
+ * in the reference. */
 int opo_get_tuning(const OpoSolver *s, int out[9]);
 
 /* Diffraction operator as one fused plane pass (Solver3D.cuh:282-323 applied at :954 and
