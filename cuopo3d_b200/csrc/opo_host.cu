@@ -1192,6 +1192,8 @@ template <typename C> int autotune(OpoSolver *s)
 bool valid_grid(int n) { return n >= 4; }
 // x / y extent: >= 4, or 1 without diffraction (the plane-wave 1-D solver)
 bool valid_extent(int n, unsigned flags) { return n >= 4 || (n == 1 && !(flags & OPO_DIFFRACTION)); }
+// The pass kernels index a field with 32-bit arithmetic: at most 2^31 - 1 voxels.
+bool valid_volume(int nx, int ny, int nt) { return (unsigned long long)nx * ny * nt <= 0x7fffffffull; }
 
 }  // namespace
 
@@ -1222,7 +1224,8 @@ int opo_crystal_dispersion(int crystal, double T, double L, double out[4])
 int opo_params_from_config(const OpoConfig *c, OpoParams *o, double *sc)
 {
     if (!c || !o) return OPO_ERR_INVALID;
-    if (!valid_extent(c->nx, c->flags) || !valid_extent(c->ny, c->flags) || !valid_grid(c->nt) || c->nz < 2)
+    if (!valid_extent(c->nx, c->flags) || !valid_extent(c->ny, c->flags) || !valid_grid(c->nt) || c->nz < 2 ||
+        !valid_volume(c->nx, c->ny, c->nt))
         return OPO_ERR_INVALID;
     if (c->precision != OPO_FP32 && c->precision != OPO_FP64) return OPO_ERR_INVALID;
     CrystalModel m;
@@ -1383,7 +1386,8 @@ static int create_impl(const OpoParams *p, const double *w, const opo::PassVaria
     *out = nullptr;
     if (!p || !w) return OPO_ERR_INVALID;
     if (p->precision != OPO_FP32 && p->precision != OPO_FP64) return OPO_ERR_INVALID;
-    if (!valid_extent(p->nx, p->flags) || !valid_extent(p->ny, p->flags) || !valid_grid(p->nt) || p->n_steps < 1)
+    if (!valid_extent(p->nx, p->flags) || !valid_extent(p->ny, p->flags) || !valid_grid(p->nt) || p->n_steps < 1 ||
+        !valid_volume(p->nx, p->ny, p->nt))
         return OPO_ERR_INVALID;
     OpoSolver *s = new (std::nothrow) OpoSolver();
     if (!s) return OPO_ERR_NOMEM;

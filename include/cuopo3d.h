@@ -81,7 +81,8 @@ typedef struct OpoConfig {
     double lp, ls;                     /* pump, signal wavelength (um); li = ls lp/(ls-lp) */
     int nx, ny, nt, nz;                /* grid; nz slices, dz = Lcr/(nz-1); nx = ny = 1 without
                                           OPO_DIFFRACTION is the plane-wave 1-D solver
-                                          (Solver1D.cuh), nt up to one tile per CTA     */
+                                          (Solver1D.cuh), nt up to one tile per CTA;
+                                          nx ny nt <= 2^31 - 1                           */
     double dQ;                         /* um/V; <= 0 keeps the crystal's 2 d33/pi          */
     double alpha[3];                   /* 1/um; < 0 keeps the crystal's value              */
     double Lcav, Rs, Ri;               /* cavity length (um); mirror reflectivities        */

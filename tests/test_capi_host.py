@@ -90,10 +90,16 @@ def test_crystal_dispersion_api():
 
 
 @pytest.mark.parametrize("bad", [dict(nx=2), dict(nt=0), dict(nz=1), dict(ls=0.4), dict(crystal=7),
-                                 dict(precision=3)])
+                                 dict(precision=3), dict(nx=2048, ny=2048, nt=1024)])  # 2^32 voxels
 def test_invalid_configs_rejected(bad):
     with pytest.raises(co.OpoError):
         co.derive(co.make_config(**bad))
+
+
+def test_largest_volume_accepted():
+    """2^31 - 1 voxels is the largest grid the 32-bit field indexing takes."""
+    p, _ = co.derive(co.make_config(nx=1024, ny=1024, nt=2047))
+    assert p.nx * p.ny * p.nt < 2 ** 31
 
 
 def test_zloop_step_counts():
