@@ -251,6 +251,12 @@ def run_ours(args):
         main = out["fp64"]
         t = main["passes"].get("t")
         achieved = V * 96 / (t["avg_us"] * 1e-6) / 1e9 if t else None
+        # The t-pass's second bound, the FP64 pipe: 558 flops per voxel (two RK4 half steps
+        # of 150 flops, three 256-point transform pairs at 5 N log2 N each way plus the phase
+        # multiply, 86 flops per field) against the device's measured FMA throughput.
+        fp64_peak = co.fp64_peak()
+        flops_t = V * 558.0
+        ach_tf = flops_t / (t["avg_us"] * 1e-6) / 1e12 if t else None
         line = {
             "metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": main["ms_per_step"],
@@ -269,6 +275,10 @@ def run_ours(args):
                          "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
                          "traffic": ncu_traffic("tpass", "fp64"),
                          "alg_bytes_per_launch": V * 96},
+            "roofline_fp64_pipe": {"bound": "fp64", "kernel": "tpass_kernel<double2>", "achieved": ach_tf,
+                                   "peak": fp64_peak, "peak_kind": "measured (opo_fp64_peak: FMA chains)",
+                                   "unit": "TFLOP/s", "frac": (ach_tf / fp64_peak) if ach_tf else None,
+                                   "alg_flops_per_launch": flops_t},
             "passes_fp64": main["passes"],
             "tuning_fp64": main["tuning"],
             "fp32": {"value": out["fp32"]["value"], "ms_per_step": out["fp32"]["ms_per_step"],

@@ -77,6 +77,7 @@ def lib():
         L.opo_params_from_config.argtypes = [ctypes.POINTER(OpoConfig), ctypes.POINTER(OpoParams), dp]
         L.opo_crystal_dispersion.argtypes = [_i, _d, _d, dp]
         L.opo_crystal_dispersion_pol.argtypes = [_i, _d, _i, _d, dp]
+        L.opo_fp64_peak.argtypes = [dp]
         L.opo_time_freq.argtypes = [_i, _d, dp, dp]
         L.opo_pump_field.argtypes = [ctypes.POINTER(OpoConfig), dp]
         L.opo_noise.argtypes = [ctypes.c_uint64, _d, ctypes.c_size_t, dp]
@@ -156,6 +157,15 @@ def make_config(**kw):
         else:
             setattr(c, k, v)
     return c
+
+
+def fp64_peak():
+    """Measured FP64 FMA throughput of the current device (TFLOP/s)."""
+    out = np.zeros(1)
+    rc = lib().opo_fp64_peak(_dptr(out))
+    if rc:
+        raise OpoError(rc, "opo_fp64_peak")
+    return float(out[0])
 
 
 def derive(cfg):

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libcuopo3d.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in ("ssfm_kernels.cu", "opo_host.cu", "noalloc_sums.cu", "batch.cu",
-                                                             "init_fields.cu", "serve.cpp", "plane_pass.cu", "ws_pass.cu")]
+                                                             "init_fields.cu", "serve.cpp", "plane_pass.cu", "ws_pass.cu", "peaks.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fft_radix.cuh", "opo_internal.h", "pass_body.cuh",
                                                    "solver_internal.h")] + [
     os.path.join(ROOT, "include", "cuopo3d.h")]

@@ -265,6 +265,11 @@ int opo_get_stream(const OpoSolver *s, void **stream);
 int opo_field_sums_noalloc(const void *f0, const void *f1, const void *f2, size_t n, int precision,
                            void *stream, double sums[3]);
 
+/* Measured FP64 arithmetic peak of the current device in TFLOP/s (independent FMA chains
+ * on every SM, best of five event-timed launches; allocates a few bytes).  The reference
+ * has no counterpart: it is the denominator of the t-pass's FP64-pipe roofline. */
+int opo_fp64_peak(double *tflops);
+
 int opo_synchronize(OpoSolver *s);
 int opo_round_trip_index(const OpoSolver *s);
 /* Number of kernels this solver has launched since creation (graph nodes included). */

@@ -309,3 +309,10 @@ def test_full_size_fp32_vs_fp64_round_trip():
     _, o32 = run_lib(co.make_config(precision=co.FP32, **kw), s0, s0, "opo", 1)
     for a, b in zip(o32, o64):
         assert rel_l2(a, b) < 2e-5
+
+
+def test_fp64_peak_probe_is_plausible():
+    """The measured FP64 FMA throughput (the t-pass's second roofline denominator) lies
+    between a tenth and twice the part's nominal 40 TFLOP/s."""
+    tf = co.fp64_peak()
+    assert 4.0 < tf < 80.0, tf
