@@ -546,7 +546,7 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     std::vector<cd> tw;
     int r1 = v.r1;
     if (fp64 && kind == kT && r1 > 8) r1 = 8;  // 3 fields x r1 complex128 live in registers
-    while (r1 >= 4 && !build_plan(n, r1, opo::max_radix(fp64, opo::consumer_threads(v)), pc.plan, tw)) r1 /= 2;
+    while (r1 >= 4 && !build_plan(n, r1, opo::variant_max_radix(fp64, v), pc.plan, tw)) r1 /= 2;
     if (r1 < 4) return fail(s, OPO_ERR_INVALID, "grid sizes must be 2^a 3^b and >= 8");
     pc.v.r1 = r1;
     const unsigned nxy = (unsigned)nx * ny;

@@ -148,6 +148,8 @@ struct PassVariant {
 inline bool is_ws(PassVariant v) { return v.threads == 160 || v.threads == 288; }
 inline int consumer_threads(PassVariant v) { return is_ws(v) ? v.threads - 32 : v.threads; }
 inline int max_radix(bool fp64, int threads) { return (fp64 && threads == 128) ? 8 : 16; }
+// Largest radix of a variant: the warp-specialised kernels always take radix 16.
+inline int variant_max_radix(bool fp64, PassVariant v) { return is_ws(v) ? 16 : max_radix(fp64, v.threads); }
 bool ws_variant_compiled(bool fp64, bool tpass, PassVariant consumers);
 
 // Whether (threads, r1) is one of the compiled variants (OPO_T_VARIANTS / OPO_A_VARIANTS

@@ -249,13 +249,14 @@ __global__ void __launch_bounds__(NC + 32, NC == 128 ? 2 : 1)
 
 // ---------------------------------------------------------------------------------
 // Compiled variants (element type, consumer threads, first-stage radix, largest radix).
+// Consumer warps have 168-204 registers, so every variant allows radix-16 stages.
 
 #define OPO_WS_T_VARIANTS(X)                                                                        \
-    X(float2, 128, 4, 16) X(float2, 256, 4, 16) X(float2, 256, 8, 16) X(double2, 128, 4, 8)          \
+    X(float2, 128, 4, 16) X(float2, 256, 4, 16) X(float2, 256, 8, 16) X(double2, 128, 4, 16)         \
     X(double2, 256, 4, 16) X(double2, 256, 8, 16)
 #define OPO_WS_A_VARIANTS(X)                                                                        \
-    X(float2, 128, 8, 16) X(float2, 128, 16, 16) X(float2, 256, 16, 16) X(double2, 128, 4, 8)        \
-    X(double2, 128, 8, 8) X(double2, 256, 8, 16)
+    X(float2, 128, 8, 16) X(float2, 128, 16, 16) X(float2, 256, 16, 16) X(double2, 128, 4, 16)       \
+    X(double2, 128, 8, 16) X(double2, 256, 8, 16)
 
 cudaError_t configure_ws_kernels(size_t smem)
 {
