@@ -287,11 +287,11 @@ def run_ours(args):
         }
         if not args.no_forms:
             tun = out["fp32"]["tuning"]
-            line["batched"] = batched_leg(co, tun)
+            line["batched"] = batched_leg(co, tun, n_inst=args.batched_instances)
             # arrival rate at ~85 % of capacity: throughput / mean work of a request
             mean_vox = (64 * 64 * 128 + 128 * 128 * 256 + 96 * 96 * 192) / 3.0
             rate = 0.85 * line["batched"]["value"] / (mean_vox * 100 * 15)
-            line["served"] = served_leg(co, tun, rate)
+            line["served"] = served_leg(co, tun, rate, n_req=args.served_requests)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
@@ -334,7 +334,7 @@ def batched_leg(co, tuning, n_inst=64, warm=1, steps=3, seed=2024):
     return {"value": vox * 100.0 * steps / (ms * 1e-3), "unit": UNIT, "instances": n_inst,
             "voxels": vox, "round_trips_timed": steps, "ms_per_round_trip": ms / steps,
             "launches_per_round_trip": launches / steps, "precision": "fp32",
-            "workload": "64 instances, N in {32,64,128}, NT in {64,128,256}, 20 mm PPLN, 100 slices"}
+            "workload": f"{n_inst} instances, N in {{32,64,128}}, NT in {{64,128,256}}, 20 mm PPLN, 100 slices"}
 
 
 def served_leg(co, tuning, rate_per_s, n_req=40, seed=7):
@@ -439,6 +439,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and served legs")
+    ap.add_argument("--batched-instances", type=int, default=64, help="instances of the batched leg")
+    ap.add_argument("--served-requests", type=int, default=40, help="requests of the served leg's sample")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup) if args.impl == "ours" else args.warmup
     if args.impl == "reference":
