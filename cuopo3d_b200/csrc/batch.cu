@@ -70,7 +70,11 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 4 : 1)
             __syncthreads();
             cur = i;
         }
-        tpass_tile<C, R1, THREADS, RMAX>(*d, gt - __ldg(prefix + i), sm);
+        // stage the tile with cp.async first, as the single-instance t-pass does
+        const unsigned tile = gt - __ldg(prefix + i);
+        const C *src[3] = {d->psrc, d->f[1], d->f[2]};
+        stage_tile<C, THREADS, false>(d->g, (unsigned)d->plan.n, tile, src, tpass_load_mask(*d), sm);
+        tpass_tile<C, R1, THREADS, RMAX, true>(*d, tile, sm);
     }
 }
 
