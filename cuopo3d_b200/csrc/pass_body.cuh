@@ -120,29 +120,32 @@ __device__ __forceinline__ int field_id(unsigned mask, int f)
 template <typename C, int R, int S, bool DIT, int THREADS>
 __device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv &fq, const C *tw, unsigned mask)
 {
+    // per item: the index arithmetic once, then every field in mask
     const unsigned q = fq.d, nl = (unsigned)g.nlines, lsl = g.lsl, lsj = g.lsj;
     const unsigned items = (unsigned)(n / R) * nl;
-    const int nf = __popc(mask);
-    for (int f = 0; f < nf; f++) {
-        C *sf = sm + (size_t)field_id(mask, f) * g.region;
-        for (unsigned w = threadIdx.x; w < items; w += THREADS) {
-            const unsigned b = fdiv(g.nl, w), l = w - b * nl;
-            const unsigned gq = fdiv(fq, b), j = b - gq * q;
-            C *s = sf + l * lsl + (gq * L + j) * lsj;
+    for (unsigned w = threadIdx.x; w < items; w += THREADS) {
+        const unsigned b = fdiv(g.nl, w), l = w - b * nl;
+        const unsigned gq = fdiv(fq, b), j = b - gq * q;
+        const unsigned off = l * lsl + (gq * L + j) * lsj;
+        const C *tj = tw + j;
+#pragma unroll 1
+        for (int f = 0; f < 3; f++) {
+            if (!(mask & (1u << f))) continue;
+            C *sp = sm + (size_t)f * g.region + off;
             C x[R];
 #pragma unroll
-            for (int m = 0; m < R; m++) x[m] = s[m * q * lsj];
+            for (int m = 0; m < R; m++) x[m] = sp[m * q * lsj];
             if (DIT && q > 1) {
 #pragma unroll
-                for (int m = 1; m < R; m++) x[m] = twmul<S>(x[m], __ldg(tw + (m - 1) * q + j));
+                for (int m = 1; m < R; m++) x[m] = twmul<S>(x[m], __ldg(tj + (m - 1) * q));
             }
             dft<R, S>(x);
             if (!DIT && q > 1) {
 #pragma unroll
-                for (int k = 1; k < R; k++) x[k] = twmul<S>(x[k], __ldg(tw + (k - 1) * q + j));
+                for (int k = 1; k < R; k++) x[k] = twmul<S>(x[k], __ldg(tj + (k - 1) * q));
             }
 #pragma unroll
-            for (int k = 0; k < R; k++) s[k * q * lsj] = x[k];
+            for (int k = 0; k < R; k++) sp[k * q * lsj] = x[k];
         }
     }
 }
@@ -154,24 +157,23 @@ __device__ void fused_middle(C *sm, const TileGeom &g, int n, const typename Tab
 {
     const unsigned nl = (unsigned)g.nlines, lsl = g.lsl, lsj = g.lsj;
     const unsigned items = (unsigned)(n / R) * nl;
-    const int nf = __popc(mask);
-    for (int f = 0; f < nf; f++) {
-        const int fid = field_id(mask, f);
-        C *sf = sm + (size_t)fid * g.region;
-        const typename TabOf<C>::type *tf = tab[fid];
-        for (unsigned w = threadIdx.x; w < items; w += THREADS) {
-            const unsigned g0 = fdiv(g.nl, w), l = w - g0 * nl;
-            C *s = sf + l * lsl + g0 * R * lsj;
-            const typename TabOf<C>::type *tb = tf + g0 * R;
+    for (unsigned w = threadIdx.x; w < items; w += THREADS) {
+        const unsigned g0 = fdiv(g.nl, w), l = w - g0 * nl;
+        const unsigned off = l * lsl + g0 * R * lsj;
+#pragma unroll 1
+        for (int f = 0; f < 3; f++) {
+            if (!(mask & (1u << f))) continue;
+            C *sp = sm + (size_t)f * g.region + off;
+            const typename TabOf<C>::type *tb = tab[f] + g0 * R;
             C x[R];
 #pragma unroll
-            for (int m = 0; m < R; m++) x[m] = s[m * lsj];
+            for (int m = 0; m < R; m++) x[m] = sp[m * lsj];
             dft<R, SF>(x);
 #pragma unroll
             for (int k = 0; k < R; k++) x[k] = tab_mul(x[k], __ldg(tb + k));
             dft<R, -SF>(x);
 #pragma unroll
-            for (int k = 0; k < R; k++) s[k * lsj] = x[k];
+            for (int k = 0; k < R; k++) sp[k * lsj] = x[k];
         }
     }
 }
@@ -228,34 +230,35 @@ __device__ __forceinline__ void middle_stages(C *sm, const TileGeom &g, const Ax
     }
 }
 
-// Last inverse stage (radix R1, stride q) of every field in mask, written to global.
+// Last inverse stage (radix R1, stride q) of every field in mask, written to global:
+// per item the index arithmetic once, then each field.
 template <typename C, int R1, int SB, bool BFAST, int THREADS>
 __device__ __forceinline__ void final_stage(C *sm, const TileGeom &g, unsigned n, unsigned base, C *const *dst,
                                             const C *tw, const FastDiv &fq0, unsigned mask)
 {
     const unsigned q = n / R1, nl = (unsigned)g.nlines, items = q * nl;
-    const int nf = __popc(mask);
-    for (int f = 0; f < nf; f++) {
-        const int fid = field_id(mask, f);
-        const C *sf = sm + (size_t)fid * g.region;
-        C *df = dst[fid] + base;
-        for (unsigned w = threadIdx.x; w < items; w += THREADS) {
-            unsigned b, l;
-            if (BFAST) {
-                l = fdiv(fq0, w);
-                b = w - l * q;
-            } else {
-                b = fdiv(g.nl, w);
-                l = w - b * nl;
-            }
-            const C *s = sf + l * g.lsl + b * g.lsj;
+    for (unsigned w = threadIdx.x; w < items; w += THREADS) {
+        unsigned b, l;
+        if (BFAST) {
+            l = fdiv(fq0, w);
+            b = w - l * q;
+        } else {
+            b = fdiv(g.nl, w);
+            l = w - b * nl;
+        }
+        const unsigned soff = l * g.lsl + b * g.lsj, goff = base + l * g.gs_l + b * g.gs_j;
+        const C *tb = tw + b;
+#pragma unroll 1
+        for (int f = 0; f < 3; f++) {
+            if (!(mask & (1u << f))) continue;
+            const C *sp = sm + (size_t)f * g.region + soff;
             C x[R1];
 #pragma unroll
-            for (int m = 0; m < R1; m++) x[m] = s[m * q * g.lsj];
+            for (int m = 0; m < R1; m++) x[m] = sp[m * q * g.lsj];
 #pragma unroll
-            for (int m = 1; m < R1; m++) x[m] = twmul<SB>(x[m], __ldg(tw + (m - 1) * q + b));
+            for (int m = 1; m < R1; m++) x[m] = twmul<SB>(x[m], __ldg(tb + (m - 1) * q));
             dft<R1, SB>(x);
-            C *d = df + l * g.gs_l + b * g.gs_j;
+            C *d = dst[f] + goff;
 #pragma unroll
             for (int k = 0; k < R1; k++) d[k * q * g.gs_j] = x[k];
         }
