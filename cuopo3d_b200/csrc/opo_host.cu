@@ -572,10 +572,27 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
         g.lsl = (unsigned)(nx + 1); g.lsj = 1; g.region = (unsigned)(rows * (nx + 1));
         g.tdiv = make_fastdiv(1); g.tmulA = 0; g.tmulB = (unsigned)rows * nx; g.gs_j = 1; g.gs_l = nx;
     }
+    const bool ws = opo::is_ws(v);
+    if (kind != kX && !ws && g.lsj * sizeof(C) < (fp64 ? 128u : 64u)) {
+        // Line groups narrower than a shared-memory wavefront: the last forward stage's
+        // butterflies (R rows apart, R its radix) would all fall on the same banks, so
+        // one padding row follows every R rows.  Every earlier stage has a stride that
+        // is a multiple of R, so its addressing stays affine.  FP32 line groups of 64 B
+        // stay unpadded: that t-pass is issue-bound, and the index arithmetic and the
+        // L1 space the padding takes cost more than the 2-way conflicts of that one
+        // stage.  (The warp-specialised kernels keep the unpadded tile their tensor
+        // copies write.)
+        const int R = pc.plan.radix[pc.plan.ns - 1];
+        if (R >= 2 && (R & (R - 1)) == 0) {
+            unsigned sh = 0;
+            while ((1 << sh) < R) sh++;
+            g.psh = sh;
+            g.region = (unsigned)(n + (n >> sh)) * g.lsj;
+        }
+    }
     g.nl = make_fastdiv((unsigned)g.nlines);
     g.rowlen = make_fastdiv((unsigned)nx);
     g.region = (g.region + 1u) & ~1u;  // keeps every field region 16-byte aligned
-    const bool ws = opo::is_ws(v);
     if (ws) {
         // tensor / bulk copies land on 128-byte boundaries
         const unsigned per128 = (unsigned)(128 / sizeof(C));

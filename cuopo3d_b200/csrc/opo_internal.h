@@ -44,8 +44,8 @@ struct AxisPlan {
 // Placement of one tile of lines.  Line l, element j of tile `tile` is the global
 // element  base(tile) + j * gs_j + l * gs_l  with
 //   base(tile) = (tile % tdiv) * tmulA + (tile / tdiv) * tmulB,
-// and lives in shared memory at  l * lsl + j * lsj  of its field's region (`region`
-// elements per field).  t and y tiles keep the global order (lines contiguous: lsl = 1,
+// and lives in shared memory at  l * lsl + (j + (j >> psh)) * lsj  of its field's
+// region (`region` elements per field).  t and y tiles keep the global order (lines contiguous: lsl = 1,
 // lsj = nlines); x tiles are rows stored row by row with an odd padded row stride
 // (lsj = 1, lsl = nx + 1), so every stage's accesses are bank-conflict free.
 struct TileGeom {
@@ -58,6 +58,9 @@ struct TileGeom {
     unsigned tmulA, tmulB;
     unsigned gs_j, gs_l;
     int pairs;       // t / y tiles: line pairs start 16-byte aligned (FP32 staging by 16 B)
+    // t / y tiles: element j of a line sits at row j + (j >> psh) (one padding row of lsj
+    // elements after every 2^psh rows, 2^psh the radix of the last forward stage); 31: none.
+    unsigned psh = 31;
 };
 
 template <typename C> struct RealOf;

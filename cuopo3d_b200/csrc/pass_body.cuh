@@ -40,6 +40,15 @@ __device__ __forceinline__ unsigned tile_base(const TileGeom &g, unsigned tile)
     return (tile - hi * g.tdiv.d) * g.tmulA + hi * g.tmulB;
 }
 
+// Shared-memory row of element j of a line (padding rows included), and the row stride
+// of a stage of stride q.  Every stage but the last forward one has q a multiple of
+// 2^psh, so row(j0 + m q) = row(j0) + m qrow(q); the last forward stage (q = 1, radix
+// 2^psh) reads row(g0 R + m) = g0 (R + 1) + m, so consecutive butterflies alternate
+// between the two halves of the shared-memory banks when a line group is narrower than
+// a wavefront.
+__device__ __forceinline__ unsigned prow(const TileGeom &g, unsigned j) { return j + (j >> g.psh); }
+__device__ __forceinline__ unsigned qrow(const TileGeom &g, unsigned q) { return q + (q >> g.psh); }
+
 // ---------------------------------------------------------------------------------
 // Tile staging with cp.async: every thread issues its share of the whole tile (all
 // fields) as asynchronous global -> shared copies, so a tile costs one memory latency
@@ -58,8 +67,8 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // Copy the raw lines of tile `tile` of the fields in mask (field f from src[f]) into their
 // shared-memory regions: t / y tiles element e = j nlines + l (lines contiguous in global
-// memory, two at a time when g.pairs), x tiles element e = l nx + j (rows contiguous),
-// placed at l lsl + j.
+// memory, two at a time when g.pairs) placed at l + prow(j) lsj, x tiles element
+// e = l nx + j (rows contiguous) placed at l lsl + j.
 template <typename C, int THREADS, bool ROWMAJOR>
 __device__ __forceinline__ void stage_tile(const TileGeom &g, unsigned n, unsigned tile, const C *const *src,
                                            unsigned mask, C *sm)
@@ -79,12 +88,12 @@ __device__ __forceinline__ void stage_tile(const TileGeom &g, unsigned n, unsign
         } else if (sizeof(C) == 8 && g.pairs) {
             for (unsigned e = 2 * threadIdx.x; e < count; e += 2 * THREADS) {
                 const unsigned j = fdiv(g.nl, e), l = e - j * g.nlines;
-                cp_async<16>(dst + l + j * g.lsj, gsrc + j * g.gs_j + l);
+                cp_async<16>(dst + l + prow(g, j) * g.lsj, gsrc + j * g.gs_j + l);
             }
         } else {
             for (unsigned e = threadIdx.x; e < count; e += THREADS) {
                 const unsigned j = fdiv(g.nl, e), l = e - j * g.nlines;
-                cp_async<sizeof(C)>(dst + l + j * g.lsj, gsrc + j * g.gs_j + l);
+                cp_async<sizeof(C)>(dst + l + prow(g, j) * g.lsj, gsrc + j * g.gs_j + l);
             }
         }
     }
@@ -121,12 +130,12 @@ template <typename C, int R, int S, bool DIT, int THREADS>
 __device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv &fq, const C *tw, unsigned mask)
 {
     // per item: the index arithmetic once, then every field in mask
-    const unsigned q = fq.d, nl = (unsigned)g.nlines, lsl = g.lsl, lsj = g.lsj;
+    const unsigned q = fq.d, nl = (unsigned)g.nlines, lsl = g.lsl, lsj = g.lsj, qs = qrow(g, q) * lsj;
     const unsigned items = (unsigned)(n / R) * nl;
     for (unsigned w = threadIdx.x; w < items; w += THREADS) {
         const unsigned b = fdiv(g.nl, w), l = w - b * nl;
         const unsigned gq = fdiv(fq, b), j = b - gq * q;
-        const unsigned off = l * lsl + (gq * L + j) * lsj;
+        const unsigned off = l * lsl + prow(g, gq * L + j) * lsj;
         const C *tj = tw + j;
 #pragma unroll 1
         for (int f = 0; f < 3; f++) {
@@ -134,7 +143,7 @@ __device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv
             C *sp = sm + (size_t)f * g.region + off;
             C x[R];
 #pragma unroll
-            for (int m = 0; m < R; m++) x[m] = sp[m * q * lsj];
+            for (int m = 0; m < R; m++) x[m] = sp[m * qs];
             if (DIT && q > 1) {
 #pragma unroll
                 for (int m = 1; m < R; m++) x[m] = twmul<S>(x[m], __ldg(tj + (m - 1) * q));
@@ -145,7 +154,7 @@ __device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv
                 for (int k = 1; k < R; k++) x[k] = twmul<S>(x[k], __ldg(tj + (k - 1) * q));
             }
 #pragma unroll
-            for (int k = 0; k < R; k++) sp[k * q * lsj] = x[k];
+            for (int k = 0; k < R; k++) sp[k * qs] = x[k];
         }
     }
 }
@@ -159,7 +168,7 @@ __device__ void fused_middle(C *sm, const TileGeom &g, int n, const typename Tab
     const unsigned items = (unsigned)(n / R) * nl;
     for (unsigned w = threadIdx.x; w < items; w += THREADS) {
         const unsigned g0 = fdiv(g.nl, w), l = w - g0 * nl;
-        const unsigned off = l * lsl + g0 * R * lsj;
+        const unsigned off = l * lsl + g0 * qrow(g, R) * lsj;
 #pragma unroll 1
         for (int f = 0; f < 3; f++) {
             if (!(mask & (1u << f))) continue;
@@ -236,7 +245,7 @@ template <typename C, int R1, int SB, bool BFAST, int THREADS>
 __device__ __forceinline__ void final_stage(C *sm, const TileGeom &g, unsigned n, unsigned base, C *const *dst,
                                             const C *tw, const FastDiv &fq0, unsigned mask)
 {
-    const unsigned q = n / R1, nl = (unsigned)g.nlines, items = q * nl;
+    const unsigned q = n / R1, nl = (unsigned)g.nlines, items = q * nl, qs = qrow(g, q) * g.lsj;
     for (unsigned w = threadIdx.x; w < items; w += THREADS) {
         unsigned b, l;
         if (BFAST) {
@@ -246,7 +255,7 @@ __device__ __forceinline__ void final_stage(C *sm, const TileGeom &g, unsigned n
             b = fdiv(g.nl, w);
             l = w - b * nl;
         }
-        const unsigned soff = l * g.lsl + b * g.lsj, goff = base + l * g.gs_l + b * g.gs_j;
+        const unsigned soff = l * g.lsl + prow(g, b) * g.lsj, goff = base + l * g.gs_l + b * g.gs_j;
         const C *tb = tw + b;
 #pragma unroll 1
         for (int f = 0; f < 3; f++) {
@@ -254,7 +263,7 @@ __device__ __forceinline__ void final_stage(C *sm, const TileGeom &g, unsigned n
             const C *sp = sm + (size_t)f * g.region + soff;
             C x[R1];
 #pragma unroll
-            for (int m = 0; m < R1; m++) x[m] = sp[m * q * g.lsj];
+            for (int m = 0; m < R1; m++) x[m] = sp[m * qs];
 #pragma unroll
             for (int m = 1; m < R1; m++) x[m] = twmul<SB>(x[m], __ldg(tb + (m - 1) * q));
             dft<R1, SB>(x);
@@ -373,7 +382,7 @@ __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile,
 {
     const AxisPlan &p = a.plan;
     const TileGeom &g = a.g;
-    const unsigned n = p.n, q = n / R1, P = g.nlines, lsj = g.lsj;
+    const unsigned n = p.n, q = n / R1, P = g.nlines, lsj = g.lsj, qs = qrow(g, q) * lsj;
     const unsigned base = tile_base(g, tile);
     bool xform = a.tmask != 0;
     if (a.skip_rows && base >= a.nx) xform = false;  // row y = base / nx != 0
@@ -390,7 +399,7 @@ __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile,
             const C *gsrc = f == 0 ? a.psrc : a.f[f];
 #pragma unroll
             for (int m = 0; m < R1; m++)
-                x[f][m] = STAGED ? sm[f * g.region + l + (b + m * q) * lsj] : gsrc[gb + m * gstep];
+                x[f][m] = STAGED ? sm[f * g.region + l + prow(g, b) * lsj + m * qs] : gsrc[gb + m * gstep];
         }
         for (int h = 0; h < a.n_rk4; h++) {
 #pragma unroll
@@ -410,9 +419,9 @@ __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile,
                 dft<R1, +1>(x[f]);
 #pragma unroll
                 for (int k = 1; k < R1; k++) x[f][k] = twmul<+1>(x[f][k], __ldg(a.tw + (k - 1) * q + b));
-                C *s = sm + (size_t)f * g.region + l + b * lsj;
+                C *s = sm + (size_t)f * g.region + l + prow(g, b) * lsj;
 #pragma unroll
-                for (int k = 0; k < R1; k++) s[k * q * lsj] = x[f][k];
+                for (int k = 0; k < R1; k++) s[k * qs] = x[f][k];
             } else if (lmask & (1u << f)) {
 #pragma unroll
                 for (int m = 0; m < R1; m++) a.f[f][gb + m * gstep] = x[f][m];
@@ -437,7 +446,7 @@ __device__ __forceinline__ void axis_tile(const AxisArgs<C> &a, unsigned tile, C
 {
     const AxisPlan &p = a.plan;
     const TileGeom &g = a.g;
-    const unsigned n = p.n, q = n / R1, NL = g.nlines;
+    const unsigned n = p.n, q = n / R1, NL = g.nlines, qs = qrow(g, q) * g.lsj;
     const int nf = __popc(a.tmask);
     const unsigned items = q * NL;
     if (nf == 0) {
@@ -458,15 +467,15 @@ __device__ __forceinline__ void axis_tile(const AxisArgs<C> &a, unsigned tile, C
                 b = fdiv(g.nl, w);
                 l = w - b * NL;
             }
-            C *s = sf + l * g.lsl + b * g.lsj;
+            C *s = sf + l * g.lsl + prow(g, b) * g.lsj;
             C x[R1];
 #pragma unroll
-            for (int m = 0; m < R1; m++) x[m] = STAGED ? s[m * q * g.lsj] : srcf[l * g.gs_l + (b + m * q) * g.gs_j];
+            for (int m = 0; m < R1; m++) x[m] = STAGED ? s[m * qs] : srcf[l * g.gs_l + (b + m * q) * g.gs_j];
             dft<R1, -1>(x);
 #pragma unroll
             for (int k = 1; k < R1; k++) x[k] = twmul<-1>(x[k], __ldg(a.tw + (k - 1) * q + b));
 #pragma unroll
-            for (int k = 0; k < R1; k++) s[k * q * g.lsj] = x[k];
+            for (int k = 0; k < R1; k++) s[k * qs] = x[k];
         }
     }
     tile_sync<BAR>();
