@@ -125,21 +125,43 @@ __device__ __forceinline__ int field_id(unsigned mask, int f)
 
 // ---------------------------------------------------------------------------------
 // Shared-memory stages.  Per field, work item w -> (line l fastest, butterfly b).
+//
+// for_items runs body(w, fields) over every item of every field in mask.  A thread takes
+// whole items and runs all their fields (the index arithmetic of an item is done once).
+// With SPREAD (the warp-specialised kernels, whose 128 / 256 consumer threads often
+// outnumber a stage's items), when that would not load every thread evenly -- the most
+// butterflies one thread runs, nf * ceil(items / THREADS), exceeds
+// ceil(nf * items / THREADS) -- the (field, item) pairs are spread over the threads
+// instead.  The other kernels compile the first form only: the second, even unused,
+// costs them 3-7 %.
+template <int THREADS, bool SPREAD, typename F>
+__device__ __forceinline__ void for_items(unsigned items, unsigned mask, F &&body)
+{
+    const unsigned nf = __popc(mask);
+    if (!SPREAD || nf * ((items + THREADS - 1) / THREADS) <= (nf * items + THREADS - 1) / THREADS) {
+        for (unsigned w = threadIdx.x; w < items; w += THREADS) body(w, mask);
+    } else if constexpr (SPREAD) {
+        for (unsigned u = threadIdx.x; u < nf * items; u += THREADS) {
+            const unsigned fi = (u >= items) + (u >= 2 * items);
+            body(u - fi * items, 1u << field_id(mask, (int)fi));
+        }
+    }
+}
 
-template <typename C, int R, int S, bool DIT, int THREADS>
+template <typename C, int R, int S, bool DIT, int THREADS, bool SPREAD = false>
 __device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv &fq, const C *tw, unsigned mask)
 {
     // per item: the index arithmetic once, then every field in mask
     const unsigned q = fq.d, nl = (unsigned)g.nlines, lsl = g.lsl, lsj = g.lsj, qs = qrow(g, q) * lsj;
     const unsigned items = (unsigned)(n / R) * nl;
-    for (unsigned w = threadIdx.x; w < items; w += THREADS) {
+    for_items<THREADS, SPREAD>(items, mask, [&](unsigned w, unsigned fm) {
         const unsigned b = fdiv(g.nl, w), l = w - b * nl;
         const unsigned gq = fdiv(fq, b), j = b - gq * q;
         const unsigned off = l * lsl + prow(g, gq * L + j) * lsj;
         const C *tj = tw + j;
 #pragma unroll 1
         for (int f = 0; f < 3; f++) {
-            if (!(mask & (1u << f))) continue;
+            if (!(fm & (1u << f))) continue;
             C *sp = sm + (size_t)f * g.region + off;
             C x[R];
 #pragma unroll
@@ -156,22 +178,22 @@ __device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv
 #pragma unroll
             for (int k = 0; k < R; k++) sp[k * qs] = x[k];
         }
-    }
+    });
 }
 
 // Last forward stage (q = 1), phase multiply, first inverse stage, in registers.
-template <typename C, int R, int SF, int THREADS>
+template <typename C, int R, int SF, int THREADS, bool SPREAD = false>
 __device__ void fused_middle(C *sm, const TileGeom &g, int n, const typename TabOf<C>::type *const *tab,
                              unsigned mask)
 {
     const unsigned nl = (unsigned)g.nlines, lsl = g.lsl, lsj = g.lsj;
     const unsigned items = (unsigned)(n / R) * nl;
-    for (unsigned w = threadIdx.x; w < items; w += THREADS) {
+    for_items<THREADS, SPREAD>(items, mask, [&](unsigned w, unsigned fm) {
         const unsigned g0 = fdiv(g.nl, w), l = w - g0 * nl;
         const unsigned off = l * lsl + g0 * qrow(g, R) * lsj;
 #pragma unroll 1
         for (int f = 0; f < 3; f++) {
-            if (!(mask & (1u << f))) continue;
+            if (!(fm & (1u << f))) continue;
             C *sp = sm + (size_t)f * g.region + off;
             const typename TabOf<C>::type *tb = tab[f] + g0 * R;
             C x[R];
@@ -184,36 +206,36 @@ __device__ void fused_middle(C *sm, const TileGeom &g, int n, const typename Tab
 #pragma unroll
             for (int k = 0; k < R; k++) sp[k * lsj] = x[k];
         }
-    }
+    });
 }
 
-template <typename C, int S, bool DIT, int THREADS, int RMAX>
+template <typename C, int S, bool DIT, int THREADS, int RMAX, bool SPREAD = false>
 __device__ void smem_stage_dispatch(int R, C *sm, const TileGeom &g, int n, int L, const FastDiv &fq,
                                     const C *tw, unsigned mask)
 {
     switch (R) {
-    case 2: smem_stage<C, 2, S, DIT, THREADS>(sm, g, n, L, fq, tw, mask); break;
-    case 3: smem_stage<C, 3, S, DIT, THREADS>(sm, g, n, L, fq, tw, mask); break;
-    case 4: smem_stage<C, 4, S, DIT, THREADS>(sm, g, n, L, fq, tw, mask); break;
-    case 8: smem_stage<C, 8, S, DIT, THREADS>(sm, g, n, L, fq, tw, mask); break;
+    case 2: smem_stage<C, 2, S, DIT, THREADS, SPREAD>(sm, g, n, L, fq, tw, mask); break;
+    case 3: smem_stage<C, 3, S, DIT, THREADS, SPREAD>(sm, g, n, L, fq, tw, mask); break;
+    case 4: smem_stage<C, 4, S, DIT, THREADS, SPREAD>(sm, g, n, L, fq, tw, mask); break;
+    case 8: smem_stage<C, 8, S, DIT, THREADS, SPREAD>(sm, g, n, L, fq, tw, mask); break;
     case 16:
-        if constexpr (RMAX >= 16) smem_stage<C, 16, S, DIT, THREADS>(sm, g, n, L, fq, tw, mask);
+        if constexpr (RMAX >= 16) smem_stage<C, 16, S, DIT, THREADS, SPREAD>(sm, g, n, L, fq, tw, mask);
         break;
     default: break;
     }
 }
 
-template <typename C, int SF, int THREADS, int RMAX>
+template <typename C, int SF, int THREADS, int RMAX, bool SPREAD = false>
 __device__ void fused_dispatch(int R, C *sm, const TileGeom &g, int n, const typename TabOf<C>::type *const *tab,
                                unsigned mask)
 {
     switch (R) {
-    case 2: fused_middle<C, 2, SF, THREADS>(sm, g, n, tab, mask); break;
-    case 3: fused_middle<C, 3, SF, THREADS>(sm, g, n, tab, mask); break;
-    case 4: fused_middle<C, 4, SF, THREADS>(sm, g, n, tab, mask); break;
-    case 8: fused_middle<C, 8, SF, THREADS>(sm, g, n, tab, mask); break;
+    case 2: fused_middle<C, 2, SF, THREADS, SPREAD>(sm, g, n, tab, mask); break;
+    case 3: fused_middle<C, 3, SF, THREADS, SPREAD>(sm, g, n, tab, mask); break;
+    case 4: fused_middle<C, 4, SF, THREADS, SPREAD>(sm, g, n, tab, mask); break;
+    case 8: fused_middle<C, 8, SF, THREADS, SPREAD>(sm, g, n, tab, mask); break;
     case 16:
-        if constexpr (RMAX >= 16) fused_middle<C, 16, SF, THREADS>(sm, g, n, tab, mask);
+        if constexpr (RMAX >= 16) fused_middle<C, 16, SF, THREADS, SPREAD>(sm, g, n, tab, mask);
         break;
     default: break;
     }
@@ -226,14 +248,14 @@ __device__ __forceinline__ void middle_stages(C *sm, const TileGeom &g, const Ax
                               const typename TabOf<C>::type *const *tab, unsigned mask)
 {
     for (int s = 1; s < p.ns - 1; s++) {
-        smem_stage_dispatch<C, SF, false, THREADS, RMAX>(p.radix[s], sm, g, p.n, p.len[s], p.q[s],
+        smem_stage_dispatch<C, SF, false, THREADS, RMAX, (BAR > 0)>(p.radix[s], sm, g, p.n, p.len[s], p.q[s],
                                                          tw + p.twoff[s], mask);
         tile_sync<BAR>();
     }
-    fused_dispatch<C, SF, THREADS, RMAX>(p.radix[p.ns - 1], sm, g, p.n, tab, mask);
+    fused_dispatch<C, SF, THREADS, RMAX, (BAR > 0)>(p.radix[p.ns - 1], sm, g, p.n, tab, mask);
     tile_sync<BAR>();
     for (int s = p.ns - 2; s >= 1; s--) {
-        smem_stage_dispatch<C, -SF, true, THREADS, RMAX>(p.radix[s], sm, g, p.n, p.len[s], p.q[s],
+        smem_stage_dispatch<C, -SF, true, THREADS, RMAX, (BAR > 0)>(p.radix[s], sm, g, p.n, p.len[s], p.q[s],
                                                          tw + p.twoff[s], mask);
         tile_sync<BAR>();
     }
@@ -241,12 +263,12 @@ __device__ __forceinline__ void middle_stages(C *sm, const TileGeom &g, const Ax
 
 // Last inverse stage (radix R1, stride q) of every field in mask, written to global:
 // per item the index arithmetic once, then each field.
-template <typename C, int R1, int SB, bool BFAST, int THREADS>
+template <typename C, int R1, int SB, bool BFAST, int THREADS, bool SPREAD = false>
 __device__ __forceinline__ void final_stage(C *sm, const TileGeom &g, unsigned n, unsigned base, C *const *dst,
                                             const C *tw, const FastDiv &fq0, unsigned mask)
 {
     const unsigned q = n / R1, nl = (unsigned)g.nlines, items = q * nl, qs = qrow(g, q) * g.lsj;
-    for (unsigned w = threadIdx.x; w < items; w += THREADS) {
+    for_items<THREADS, SPREAD>(items, mask, [&](unsigned w, unsigned fm) {
         unsigned b, l;
         if (BFAST) {
             l = fdiv(fq0, w);
@@ -259,7 +281,7 @@ __device__ __forceinline__ void final_stage(C *sm, const TileGeom &g, unsigned n
         const C *tb = tw + b;
 #pragma unroll 1
         for (int f = 0; f < 3; f++) {
-            if (!(mask & (1u << f))) continue;
+            if (!(fm & (1u << f))) continue;
             const C *sp = sm + (size_t)f * g.region + soff;
             C x[R1];
 #pragma unroll
@@ -271,7 +293,7 @@ __device__ __forceinline__ void final_stage(C *sm, const TileGeom &g, unsigned n
 #pragma unroll
             for (int k = 0; k < R1; k++) d[k * q * g.gs_j] = x[k];
         }
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------------
@@ -431,7 +453,7 @@ __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile,
     tile_sync<BAR>();
     if (!tmask) return;
     middle_stages<C, +1, THREADS, RMAX, BAR>(sm, g, p, a.tw, a.tab, tmask);
-    final_stage<C, R1, -1, false, THREADS>(sm, g, n, base, a.f, a.tw, p.q[0], tmask);
+    final_stage<C, R1, -1, false, THREADS, (BAR > 0)>(sm, g, n, base, a.f, a.tw, p.q[0], tmask);
     tile_sync<BAR>();
 }
 
@@ -480,7 +502,7 @@ __device__ __forceinline__ void axis_tile(const AxisArgs<C> &a, unsigned tile, C
     }
     tile_sync<BAR>();
     middle_stages<C, -1, THREADS, RMAX, BAR>(sm, g, p, a.tw, a.tab, a.tmask);
-    final_stage<C, R1, +1, BFAST, THREADS>(sm, g, n, base, a.f, a.tw, p.q[0], a.tmask);
+    final_stage<C, R1, +1, BFAST, THREADS, (BAR > 0)>(sm, g, n, base, a.f, a.tw, p.q[0], a.tmask);
     tile_sync<BAR>();
 }
 
