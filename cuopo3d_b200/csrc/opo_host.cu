@@ -636,6 +636,18 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
         }
         pc.smem = opo::kWsHeaderBytes + w.nstages * (size_t)w.stage_bytes;
         if (pc.smem > 227 * 1024) return fail(s, OPO_ERR_INVALID, "stage ring does not fit in shared memory");
+        if (kind != kT) {
+            // the stage twiddles and up to three phase tables go into shared memory beside
+            // the ring when that keeps as many CTAs resident per SM (228 KB per SM, 1 KB
+            // reserved per CTA); otherwise the consumers read them from global memory
+            const size_t tab_bytes = (tw.size() + 3 * (size_t)n) * sizeof(C);
+            const size_t per_sm = 228 * 1024, with = pc.smem + tab_bytes;
+            if (with <= 227 * 1024 && per_sm / (with + 1024) >= per_sm / (pc.smem + 1024)) {
+                w.tab_off = (unsigned)pc.smem;
+                w.ntw = (unsigned)tw.size();
+                pc.smem = with;
+            }
+        }
     }
 
     int rc;

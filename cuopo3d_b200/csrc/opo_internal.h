@@ -127,6 +127,7 @@ template <typename C> struct PlaneArgs {
 // flag, then nstages stages of stage_bytes.
 constexpr unsigned kWsMaxStages = 4;
 constexpr unsigned kWsHeaderBytes = 128;
+constexpr unsigned kWsTabPtrOffset = 80;  // header: three phase-table pointers (after the mbarriers and flag)
 enum { kWsTensor = 0, kWsRows = 1 };
 struct WsArgs {
     int *err;               // error word in global memory (0: no error)
@@ -139,6 +140,10 @@ struct WsArgs {
     // line_dim (2: t for the t-pass, 1: y for the y-pass); lines / box_lines boxes per field
     unsigned px, inner_mult, line_dim, lines, box_lines;
     unsigned row_bytes;     // rows mode: bytes per row copy
+    // axis passes: byte offset in dynamic shared memory where the consumers copy the stage
+    // twiddles (ntw values) and the phase tables of the transformed fields (plan.n values
+    // each) before the first tile; 0: the tables are read from global memory
+    unsigned tab_off, ntw;
 };
 
 // Kernel variant of one pass: CTA size and first-stage radix; the largest radix any

@@ -126,21 +126,32 @@ __device__ __forceinline__ int field_id(unsigned mask, int f)
 // ---------------------------------------------------------------------------------
 // Shared-memory stages.  Per field, work item w -> (line l fastest, butterfly b).
 //
-// for_items runs body(w, fields) over every item of every field in mask.  A thread takes
-// whole items and runs all their fields (the index arithmetic of an item is done once).
-// With SPREAD (the warp-specialised kernels, whose 128 / 256 consumer threads often
-// outnumber a stage's items), when that would not load every thread evenly -- the most
-// butterflies one thread runs, nf * ceil(items / THREADS), exceeds
-// ceil(nf * items / THREADS) -- the (field, item) pairs are spread over the threads
-// instead.  The other kernels compile the first form only: the second, even unused,
-// costs them 3-7 %.
-template <int THREADS, bool SPREAD, typename F>
+// The stage functions take WS = true in the warp-specialised kernels (consumer warps of
+// a CTA with a producer warp).  Two things follow from it:
+//  * for_items runs body(w, fields) over every item of every field in mask.  A thread
+//    takes whole items and runs all their fields (the index arithmetic of an item is done
+//    once).  With WS, whose 128 / 256 consumer threads often outnumber a stage's items,
+//    when that would not load every thread evenly -- the most butterflies one thread
+//    runs, nf * ceil(items / THREADS), exceeds ceil(nf * items / THREADS) -- the
+//    (field, item) pairs are spread over the threads instead.  The other kernels compile
+//    the first form only: the second, even unused, costs them 3-7 %.
+//  * ldtab<WS> reads twiddles and phase tables: __ldg from global memory, or with WS a
+//    generic load, since those kernels may hold the tables in shared memory.
+template <bool WS, typename T> __device__ __forceinline__ T ldtab(const T *p)
+{
+    if constexpr (WS)
+        return *p;
+    else
+        return __ldg(p);
+}
+
+template <int THREADS, bool WS, typename F>
 __device__ __forceinline__ void for_items(unsigned items, unsigned mask, F &&body)
 {
     const unsigned nf = __popc(mask);
-    if (!SPREAD || nf * ((items + THREADS - 1) / THREADS) <= (nf * items + THREADS - 1) / THREADS) {
+    if (!WS || nf * ((items + THREADS - 1) / THREADS) <= (nf * items + THREADS - 1) / THREADS) {
         for (unsigned w = threadIdx.x; w < items; w += THREADS) body(w, mask);
-    } else if constexpr (SPREAD) {
+    } else if constexpr (WS) {
         for (unsigned u = threadIdx.x; u < nf * items; u += THREADS) {
             const unsigned fi = (u >= items) + (u >= 2 * items);
             body(u - fi * items, 1u << field_id(mask, (int)fi));
@@ -148,13 +159,13 @@ __device__ __forceinline__ void for_items(unsigned items, unsigned mask, F &&bod
     }
 }
 
-template <typename C, int R, int S, bool DIT, int THREADS, bool SPREAD = false>
+template <typename C, int R, int S, bool DIT, int THREADS, bool WS = false>
 __device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv &fq, const C *tw, unsigned mask)
 {
     // per item: the index arithmetic once, then every field in mask
     const unsigned q = fq.d, nl = (unsigned)g.nlines, lsl = g.lsl, lsj = g.lsj, qs = qrow(g, q) * lsj;
     const unsigned items = (unsigned)(n / R) * nl;
-    for_items<THREADS, SPREAD>(items, mask, [&](unsigned w, unsigned fm) {
+    for_items<THREADS, WS>(items, mask, [&](unsigned w, unsigned fm) {
         const unsigned b = fdiv(g.nl, w), l = w - b * nl;
         const unsigned gq = fdiv(fq, b), j = b - gq * q;
         const unsigned off = l * lsl + prow(g, gq * L + j) * lsj;
@@ -168,12 +179,12 @@ __device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv
             for (int m = 0; m < R; m++) x[m] = sp[m * qs];
             if (DIT && q > 1) {
 #pragma unroll
-                for (int m = 1; m < R; m++) x[m] = twmul<S>(x[m], __ldg(tj + (m - 1) * q));
+                for (int m = 1; m < R; m++) x[m] = twmul<S>(x[m], ldtab<WS>(tj + (m - 1) * q));
             }
             dft<R, S>(x);
             if (!DIT && q > 1) {
 #pragma unroll
-                for (int k = 1; k < R; k++) x[k] = twmul<S>(x[k], __ldg(tj + (k - 1) * q));
+                for (int k = 1; k < R; k++) x[k] = twmul<S>(x[k], ldtab<WS>(tj + (k - 1) * q));
             }
 #pragma unroll
             for (int k = 0; k < R; k++) sp[k * qs] = x[k];
@@ -182,13 +193,13 @@ __device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv
 }
 
 // Last forward stage (q = 1), phase multiply, first inverse stage, in registers.
-template <typename C, int R, int SF, int THREADS, bool SPREAD = false>
+template <typename C, int R, int SF, int THREADS, bool WS = false>
 __device__ void fused_middle(C *sm, const TileGeom &g, int n, const typename TabOf<C>::type *const *tab,
                              unsigned mask)
 {
     const unsigned nl = (unsigned)g.nlines, lsl = g.lsl, lsj = g.lsj;
     const unsigned items = (unsigned)(n / R) * nl;
-    for_items<THREADS, SPREAD>(items, mask, [&](unsigned w, unsigned fm) {
+    for_items<THREADS, WS>(items, mask, [&](unsigned w, unsigned fm) {
         const unsigned g0 = fdiv(g.nl, w), l = w - g0 * nl;
         const unsigned off = l * lsl + g0 * qrow(g, R) * lsj;
 #pragma unroll 1
@@ -201,7 +212,7 @@ __device__ void fused_middle(C *sm, const TileGeom &g, int n, const typename Tab
             for (int m = 0; m < R; m++) x[m] = sp[m * lsj];
             dft<R, SF>(x);
 #pragma unroll
-            for (int k = 0; k < R; k++) x[k] = tab_mul(x[k], __ldg(tb + k));
+            for (int k = 0; k < R; k++) x[k] = tab_mul(x[k], ldtab<WS>(tb + k));
             dft<R, -SF>(x);
 #pragma unroll
             for (int k = 0; k < R; k++) sp[k * lsj] = x[k];
@@ -209,33 +220,33 @@ __device__ void fused_middle(C *sm, const TileGeom &g, int n, const typename Tab
     });
 }
 
-template <typename C, int S, bool DIT, int THREADS, int RMAX, bool SPREAD = false>
+template <typename C, int S, bool DIT, int THREADS, int RMAX, bool WS = false>
 __device__ void smem_stage_dispatch(int R, C *sm, const TileGeom &g, int n, int L, const FastDiv &fq,
                                     const C *tw, unsigned mask)
 {
     switch (R) {
-    case 2: smem_stage<C, 2, S, DIT, THREADS, SPREAD>(sm, g, n, L, fq, tw, mask); break;
-    case 3: smem_stage<C, 3, S, DIT, THREADS, SPREAD>(sm, g, n, L, fq, tw, mask); break;
-    case 4: smem_stage<C, 4, S, DIT, THREADS, SPREAD>(sm, g, n, L, fq, tw, mask); break;
-    case 8: smem_stage<C, 8, S, DIT, THREADS, SPREAD>(sm, g, n, L, fq, tw, mask); break;
+    case 2: smem_stage<C, 2, S, DIT, THREADS, WS>(sm, g, n, L, fq, tw, mask); break;
+    case 3: smem_stage<C, 3, S, DIT, THREADS, WS>(sm, g, n, L, fq, tw, mask); break;
+    case 4: smem_stage<C, 4, S, DIT, THREADS, WS>(sm, g, n, L, fq, tw, mask); break;
+    case 8: smem_stage<C, 8, S, DIT, THREADS, WS>(sm, g, n, L, fq, tw, mask); break;
     case 16:
-        if constexpr (RMAX >= 16) smem_stage<C, 16, S, DIT, THREADS, SPREAD>(sm, g, n, L, fq, tw, mask);
+        if constexpr (RMAX >= 16) smem_stage<C, 16, S, DIT, THREADS, WS>(sm, g, n, L, fq, tw, mask);
         break;
     default: break;
     }
 }
 
-template <typename C, int SF, int THREADS, int RMAX, bool SPREAD = false>
+template <typename C, int SF, int THREADS, int RMAX, bool WS = false>
 __device__ void fused_dispatch(int R, C *sm, const TileGeom &g, int n, const typename TabOf<C>::type *const *tab,
                                unsigned mask)
 {
     switch (R) {
-    case 2: fused_middle<C, 2, SF, THREADS, SPREAD>(sm, g, n, tab, mask); break;
-    case 3: fused_middle<C, 3, SF, THREADS, SPREAD>(sm, g, n, tab, mask); break;
-    case 4: fused_middle<C, 4, SF, THREADS, SPREAD>(sm, g, n, tab, mask); break;
-    case 8: fused_middle<C, 8, SF, THREADS, SPREAD>(sm, g, n, tab, mask); break;
+    case 2: fused_middle<C, 2, SF, THREADS, WS>(sm, g, n, tab, mask); break;
+    case 3: fused_middle<C, 3, SF, THREADS, WS>(sm, g, n, tab, mask); break;
+    case 4: fused_middle<C, 4, SF, THREADS, WS>(sm, g, n, tab, mask); break;
+    case 8: fused_middle<C, 8, SF, THREADS, WS>(sm, g, n, tab, mask); break;
     case 16:
-        if constexpr (RMAX >= 16) fused_middle<C, 16, SF, THREADS, SPREAD>(sm, g, n, tab, mask);
+        if constexpr (RMAX >= 16) fused_middle<C, 16, SF, THREADS, WS>(sm, g, n, tab, mask);
         break;
     default: break;
     }
@@ -263,12 +274,12 @@ __device__ __forceinline__ void middle_stages(C *sm, const TileGeom &g, const Ax
 
 // Last inverse stage (radix R1, stride q) of every field in mask, written to global:
 // per item the index arithmetic once, then each field.
-template <typename C, int R1, int SB, bool BFAST, int THREADS, bool SPREAD = false>
+template <typename C, int R1, int SB, bool BFAST, int THREADS, bool WS = false>
 __device__ __forceinline__ void final_stage(C *sm, const TileGeom &g, unsigned n, unsigned base, C *const *dst,
                                             const C *tw, const FastDiv &fq0, unsigned mask)
 {
     const unsigned q = n / R1, nl = (unsigned)g.nlines, items = q * nl, qs = qrow(g, q) * g.lsj;
-    for_items<THREADS, SPREAD>(items, mask, [&](unsigned w, unsigned fm) {
+    for_items<THREADS, WS>(items, mask, [&](unsigned w, unsigned fm) {
         unsigned b, l;
         if (BFAST) {
             l = fdiv(fq0, w);
@@ -287,7 +298,7 @@ __device__ __forceinline__ void final_stage(C *sm, const TileGeom &g, unsigned n
 #pragma unroll
             for (int m = 0; m < R1; m++) x[m] = sp[m * qs];
 #pragma unroll
-            for (int m = 1; m < R1; m++) x[m] = twmul<SB>(x[m], __ldg(tb + (m - 1) * q));
+            for (int m = 1; m < R1; m++) x[m] = twmul<SB>(x[m], ldtab<WS>(tb + (m - 1) * q));
             dft<R1, SB>(x);
             C *d = dst[f] + goff;
 #pragma unroll
@@ -440,7 +451,7 @@ __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile,
             if (tmask & (1u << f)) {
                 dft<R1, +1>(x[f]);
 #pragma unroll
-                for (int k = 1; k < R1; k++) x[f][k] = twmul<+1>(x[f][k], __ldg(a.tw + (k - 1) * q + b));
+                for (int k = 1; k < R1; k++) x[f][k] = twmul<+1>(x[f][k], ldtab<(BAR > 0)>(a.tw + (k - 1) * q + b));
                 C *s = sm + (size_t)f * g.region + l + prow(g, b) * lsj;
 #pragma unroll
                 for (int k = 0; k < R1; k++) s[k * qs] = x[f][k];
@@ -464,7 +475,8 @@ __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile,
 // index is the contiguous one); otherwise consecutive threads take consecutive lines.
 
 template <typename C, int R1, bool BFAST, int THREADS, int RMAX, bool STAGED = false, int BAR = 0>
-__device__ __forceinline__ void axis_tile(const AxisArgs<C> &a, unsigned tile, C *sm)
+__device__ __forceinline__ void axis_tile(const AxisArgs<C> &a, unsigned tile, C *sm, const C *tw,
+                                          const typename TabOf<C>::type *const *tab)
 {
     const AxisPlan &p = a.plan;
     const TileGeom &g = a.g;
@@ -495,15 +507,22 @@ __device__ __forceinline__ void axis_tile(const AxisArgs<C> &a, unsigned tile, C
             for (int m = 0; m < R1; m++) x[m] = STAGED ? s[m * qs] : srcf[l * g.gs_l + (b + m * q) * g.gs_j];
             dft<R1, -1>(x);
 #pragma unroll
-            for (int k = 1; k < R1; k++) x[k] = twmul<-1>(x[k], __ldg(a.tw + (k - 1) * q + b));
+            for (int k = 1; k < R1; k++) x[k] = twmul<-1>(x[k], ldtab<(BAR > 0)>(tw + (k - 1) * q + b));
 #pragma unroll
             for (int k = 0; k < R1; k++) s[k * qs] = x[k];
         }
     }
     tile_sync<BAR>();
-    middle_stages<C, -1, THREADS, RMAX, BAR>(sm, g, p, a.tw, a.tab, a.tmask);
-    final_stage<C, R1, +1, BFAST, THREADS, (BAR > 0)>(sm, g, n, base, a.f, a.tw, p.q[0], a.tmask);
+    middle_stages<C, -1, THREADS, RMAX, BAR>(sm, g, p, tw, tab, a.tmask);
+    final_stage<C, R1, +1, BFAST, THREADS, (BAR > 0)>(sm, g, n, base, a.f, tw, p.q[0], a.tmask);
     tile_sync<BAR>();
+}
+
+// The same with the pass's own twiddle and phase-table pointers.
+template <typename C, int R1, bool BFAST, int THREADS, int RMAX, bool STAGED = false, int BAR = 0>
+__device__ __forceinline__ void axis_tile(const AxisArgs<C> &a, unsigned tile, C *sm)
+{
+    axis_tile<C, R1, BFAST, THREADS, RMAX, STAGED, BAR>(a, tile, sm, a.tw, a.tab);
 }
 
 }  // namespace opo

@@ -242,8 +242,29 @@ __global__ void __launch_bounds__(NC + 32, NC == 128 ? 2 : 1)
         producer_loop<C>(w, a.g, a.tmask, maps, a.f, stages, full, empty);
         return;
     }
+    using TT = typename TabOf<C>::type;
+    const C *tw = a.tw;
+    const TT *const *tab = a.tab;
+    if (w.tab_off) {
+        // the pass's stage twiddles and phase tables, read by every tile, into shared
+        // memory; the three table pointers sit in the header (indexed by field at run time)
+        C *tws = reinterpret_cast<C *>(smem_raw + w.tab_off);
+        for (unsigned i = threadIdx.x; i < w.ntw; i += NC) tws[i] = a.tw[i];
+        TT *tb = reinterpret_cast<TT *>(tws + w.ntw);
+        const TT **tabs = reinterpret_cast<const TT **>(smem_raw + kWsTabPtrOffset);
+        const unsigned n = (unsigned)a.plan.n;
+        for (int f = 0; f < 3; f++) {
+            if (!(a.tmask & (1u << f))) continue;
+            for (unsigned i = threadIdx.x; i < n; i += NC) tb[i] = a.tab[f][i];
+            if (threadIdx.x == 0) tabs[f] = tb;
+            tb += n;
+        }
+        tile_sync<NC>();
+        tw = tws;
+        tab = tabs;
+    }
     consumer_loop<NC>(w, (unsigned)a.g.ntiles, full, empty, abort_flag, [&](unsigned tile, unsigned s) {
-        axis_tile<C, R1, BFAST, NC, RMAX, true, NC>(a, tile, stage_ptr<C>(stages, w, s));
+        axis_tile<C, R1, BFAST, NC, RMAX, true, NC>(a, tile, stage_ptr<C>(stages, w, s), tw, tab);
     });
 }
 
