@@ -15,6 +15,61 @@ template <> struct Cpx<double> { using type = double2; };
 
 template <typename C> __host__ __device__ __forceinline__ C cadd(C a, C b) { return C{a.x + b.x, a.y + b.y}; }
 template <typename C> __host__ __device__ __forceinline__ C csub(C a, C b) { return C{a.x - b.x, a.y - b.y}; }
+// float2: both components in one of Blackwell's packed two-lane FP32 instructions
+// (add / sub .f32x2 on a 64-bit register pair), half the issue slots of two scalar ones.
+__host__ __device__ __forceinline__ unsigned long long f2pack(float2 a)
+{
+#if defined(__CUDA_ARCH__)
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+#else
+    return 0;
+#endif
+}
+__host__ __device__ __forceinline__ float2 f2unpack(unsigned long long r)
+{
+    float2 a{0.f, 0.f};
+#if defined(__CUDA_ARCH__)
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+#endif
+    return a;
+}
+template <> __host__ __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b)
+{
+#if defined(__CUDA_ARCH__)
+    unsigned long long d;
+    asm("add.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2pack(a)), "l"(f2pack(b)));
+    return f2unpack(d);
+#else
+    return float2{a.x + b.x, a.y + b.y};
+#endif
+}
+template <> __host__ __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b)
+{
+#if defined(__CUDA_ARCH__)
+    unsigned long long d;
+    asm("sub.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2pack(a)), "l"(f2pack(b)));
+    return f2unpack(d);
+#else
+    return float2{a.x - b.x, a.y - b.y};
+#endif
+}
+// y + s x for real s
+template <typename C, typename T> __host__ __device__ __forceinline__ C caxpy(T s, C x, C y)
+{
+    return C{y.x + s * x.x, y.y + s * x.y};
+}
+template <> __host__ __device__ __forceinline__ float2 caxpy<float2, float>(float s, float2 x, float2 y)
+{
+#if defined(__CUDA_ARCH__)
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2pack(float2{s, s})), "l"(f2pack(x)), "l"(f2pack(y)));
+    return f2unpack(d);
+#else
+    return float2{y.x + s * x.x, y.y + s * x.y};
+#endif
+}
 template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b)
 {
     return C{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};

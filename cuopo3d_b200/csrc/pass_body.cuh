@@ -351,19 +351,19 @@ __device__ __forceinline__ void rk4_half_fast(const TPassArgs<C> &a, C &p, C &s,
     C Up = up, Us = us, Ui = ui;
     C p2 = add_iku(p, a.c1k[0], up), s2 = add_iku(s, a.c1k[1], us), i2 = add_iku(i, a.c1k[2], ui);
     up = cmul(s2, i2); us = cmulc(p2, i2); ui = cmulc(p2, s2);  // stage 2
-    Up = C{Up.x + T(2) * up.x, Up.y + T(2) * up.y};
-    Us = C{Us.x + T(2) * us.x, Us.y + T(2) * us.y};
-    Ui = C{Ui.x + T(2) * ui.x, Ui.y + T(2) * ui.y};
+    Up = caxpy(T(2), up, Up);
+    Us = caxpy(T(2), us, Us);
+    Ui = caxpy(T(2), ui, Ui);
     p2 = add_iku(p, a.c1k[0], up); s2 = add_iku(s, a.c1k[1], us); i2 = add_iku(i, a.c1k[2], ui);
     up = cmul(s2, i2); us = cmulc(p2, i2); ui = cmulc(p2, s2);  // stage 3
-    Up = C{Up.x + T(2) * up.x, Up.y + T(2) * up.y};
-    Us = C{Us.x + T(2) * us.x, Us.y + T(2) * us.y};
-    Ui = C{Ui.x + T(2) * ui.x, Ui.y + T(2) * ui.y};
+    Up = caxpy(T(2), up, Up);
+    Us = caxpy(T(2), us, Us);
+    Ui = caxpy(T(2), ui, Ui);
     p2 = add_iku(p, a.c3k[0], up); s2 = add_iku(s, a.c3k[1], us); i2 = add_iku(i, a.c3k[2], ui);
     up = cmul(s2, i2); us = cmulc(p2, i2); ui = cmulc(p2, s2);  // stage 4
-    Up = C{Up.x + up.x, Up.y + up.y};
-    Us = C{Us.x + us.x, Us.y + us.y};
-    Ui = C{Ui.x + ui.x, Ui.y + ui.y};
+    Up = cadd(Up, up);
+    Us = cadd(Us, us);
+    Ui = cadd(Ui, ui);
     p = add_iku(p, a.h6k[0], Up);
     s = add_iku(s, a.h6k[1], Us);
     i = add_iku(i, a.h6k[2], Ui);
