@@ -170,9 +170,8 @@ __device__ void smem_stage(C *sm, const TileGeom &g, int n, int L, const FastDiv
         const unsigned gq = fdiv(fq, b), j = b - gq * q;
         const unsigned off = l * lsl + prow(g, gq * L + j) * lsj;
         const C *tj = tw + j;
-#pragma unroll 1
-        for (int f = 0; f < 3; f++) {
-            if (!(fm & (1u << f))) continue;
+        for (unsigned fb = fm; fb; fb &= fb - 1) {
+            const int f = __ffs(fb) - 1;
             C *sp = sm + (size_t)f * g.region + off;
             C x[R];
 #pragma unroll
@@ -202,9 +201,8 @@ __device__ void fused_middle(C *sm, const TileGeom &g, int n, const typename Tab
     for_items<THREADS, WS>(items, mask, [&](unsigned w, unsigned fm) {
         const unsigned g0 = fdiv(g.nl, w), l = w - g0 * nl;
         const unsigned off = l * lsl + g0 * qrow(g, R) * lsj;
-#pragma unroll 1
-        for (int f = 0; f < 3; f++) {
-            if (!(fm & (1u << f))) continue;
+        for (unsigned fb = fm; fb; fb &= fb - 1) {
+            const int f = __ffs(fb) - 1;
             C *sp = sm + (size_t)f * g.region + off;
             const typename TabOf<C>::type *tb = tab[f] + g0 * R;
             C x[R];
@@ -290,9 +288,8 @@ __device__ __forceinline__ void final_stage(C *sm, const TileGeom &g, unsigned n
         }
         const unsigned soff = l * g.lsl + prow(g, b) * g.lsj, goff = base + l * g.gs_l + b * g.gs_j;
         const C *tb = tw + b;
-#pragma unroll 1
-        for (int f = 0; f < 3; f++) {
-            if (!(fm & (1u << f))) continue;
+        for (unsigned fb = fm; fb; fb &= fb - 1) {
+            const int f = __ffs(fb) - 1;
             const C *sp = sm + (size_t)f * g.region + soff;
             C x[R1];
 #pragma unroll
