@@ -88,6 +88,23 @@ def test_ws_1d_long_time_axis_fp64():
         assert rel_l2(a, b) < 1e-10
 
 
+def test_ws_tables_from_global_memory_fp64():
+    """A 1024-point y axis: its twiddles and phase tables (~64 KB) beside the two-stage
+    ring would leave one CTA per SM instead of two, so the consumers read them from global
+    memory instead of copying them into shared memory; same results as the classic
+    kernels and the oracle."""
+    kw = base_kw(16, 1024, 16, LY=2000.0, nz=3)
+    cfg = co.make_config(precision=co.FP64, **kw)
+    tun = tuning((128, 1024, 4), (128, 1024, 8), (160, 1024, 8))
+    sim, got = run(cfg, tun)
+    assert sim.tuning["y"]["threads"] == 160
+    _, ref_c = run(cfg, tuning((128, 1024, 4), (128, 1024, 8), (128, 1024, 8)))
+    ref_o = oracle(kw)
+    for a, b, c in zip(got, ref_c, ref_o):
+        assert rel_l2(a, b) < 1e-13
+        assert rel_l2(a, c) < 1e-10
+
+
 def test_ws_variant_refused_where_it_does_not_apply():
     # FP32 x rows of nx + 1 complex64 are not 16-byte multiples: no warp-specialised x-pass
     cfg = co.make_config(precision=co.FP32, **base_kw(32, 32, 64))
