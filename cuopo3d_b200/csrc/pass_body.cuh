@@ -333,37 +333,46 @@ __device__ __forceinline__ void cwe_rhs_phase(const T *kap, const C &ph, C p, C 
 // The products u_p = s i, u_s = p i*, u_i = p s* give k = i kappa u, so every use of k
 // (the next stage's A + c k and the final sum) folds kappa and the step weights into
 // precomputed constants: A + c k = (A.x - c kappa u.y, A.y + c kappa u.x), and
-// A += (h/6) kappa i (u1 + 2 u2 + 2 u3 + u4).
+// A += (h/6) kappa i (u1 + 2 u2 + 2 u3 + u4).  The products and their weighted sum are
+// held with their components swapped, w = (u.y, u.x), so that A + c k = A + (-c kappa,
+// c kappa) * w componentwise: one packed f32x2 fused multiply-add in FP32.
+template <typename C> __device__ __forceinline__ C swp(C u) { return C{u.y, u.x}; }
 template <typename C, typename T>
-__device__ __forceinline__ C add_iku(C a, T ck, C u)
+__device__ __forceinline__ C add_iku_w(C a, T ck, C w)
 {
-    return C{a.x - ck * u.y, a.y + ck * u.x};
+    return C{a.x - ck * w.x, a.y + ck * w.y};
+}
+template <> __device__ __forceinline__ float2 add_iku_w<float2, float>(float2 a, float ck, float2 w)
+{
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2pack(float2{-ck, ck})), "l"(f2pack(w)), "l"(f2pack(a)));
+    return f2unpack(d);
 }
 
 template <typename C>
 __device__ __forceinline__ void rk4_half_fast(const TPassArgs<C> &a, C &p, C &s, C &i)
 {
     using T = typename TPassArgs<C>::T;
-    C up = cmul(s, i), us = cmulc(p, i), ui = cmulc(p, s);  // stage 1
+    C up = swp(cmul(s, i)), us = swp(cmulc(p, i)), ui = swp(cmulc(p, s));  // stage 1
     C Up = up, Us = us, Ui = ui;
-    C p2 = add_iku(p, a.c1k[0], up), s2 = add_iku(s, a.c1k[1], us), i2 = add_iku(i, a.c1k[2], ui);
-    up = cmul(s2, i2); us = cmulc(p2, i2); ui = cmulc(p2, s2);  // stage 2
+    C p2 = add_iku_w(p, a.c1k[0], up), s2 = add_iku_w(s, a.c1k[1], us), i2 = add_iku_w(i, a.c1k[2], ui);
+    up = swp(cmul(s2, i2)); us = swp(cmulc(p2, i2)); ui = swp(cmulc(p2, s2));  // stage 2
     Up = caxpy(T(2), up, Up);
     Us = caxpy(T(2), us, Us);
     Ui = caxpy(T(2), ui, Ui);
-    p2 = add_iku(p, a.c1k[0], up); s2 = add_iku(s, a.c1k[1], us); i2 = add_iku(i, a.c1k[2], ui);
-    up = cmul(s2, i2); us = cmulc(p2, i2); ui = cmulc(p2, s2);  // stage 3
+    p2 = add_iku_w(p, a.c1k[0], up); s2 = add_iku_w(s, a.c1k[1], us); i2 = add_iku_w(i, a.c1k[2], ui);
+    up = swp(cmul(s2, i2)); us = swp(cmulc(p2, i2)); ui = swp(cmulc(p2, s2));  // stage 3
     Up = caxpy(T(2), up, Up);
     Us = caxpy(T(2), us, Us);
     Ui = caxpy(T(2), ui, Ui);
-    p2 = add_iku(p, a.c3k[0], up); s2 = add_iku(s, a.c3k[1], us); i2 = add_iku(i, a.c3k[2], ui);
-    up = cmul(s2, i2); us = cmulc(p2, i2); ui = cmulc(p2, s2);  // stage 4
+    p2 = add_iku_w(p, a.c3k[0], up); s2 = add_iku_w(s, a.c3k[1], us); i2 = add_iku_w(i, a.c3k[2], ui);
+    up = swp(cmul(s2, i2)); us = swp(cmulc(p2, i2)); ui = swp(cmulc(p2, s2));  // stage 4
     Up = cadd(Up, up);
     Us = cadd(Us, us);
     Ui = cadd(Ui, ui);
-    p = add_iku(p, a.h6k[0], Up);
-    s = add_iku(s, a.h6k[1], Us);
-    i = add_iku(i, a.h6k[2], Ui);
+    p = add_iku_w(p, a.h6k[0], Up);
+    s = add_iku_w(s, a.h6k[1], Us);
+    i = add_iku_w(i, a.h6k[2], Ui);
 }
 
 template <typename C>
