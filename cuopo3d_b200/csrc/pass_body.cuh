@@ -494,6 +494,38 @@ __device__ __forceinline__ void axis_tile(const AxisArgs<C> &a, unsigned tile, C
         return;
     }
     const unsigned base = tile_base(g, tile);
+    if constexpr (!STAGED && sizeof(C) == 8 && R1 <= 8) {
+        // FP32 first stage from global memory: every field's values of an item are loaded
+        // before any is transformed, three times the loads in flight per thread
+        for (unsigned w = threadIdx.x; w < items; w += THREADS) {
+            unsigned b, l;
+            if (BFAST) {
+                l = fdiv(p.q[0], w);
+                b = w - l * q;
+            } else {
+                b = fdiv(g.nl, w);
+                l = w - b * NL;
+            }
+            const unsigned gb = base + l * g.gs_l + b * g.gs_j, off = l * g.lsl + prow(g, b) * g.lsj;
+            C x[3][R1];
+#pragma unroll
+            for (int f = 0; f < 3; f++) {
+                if (!(a.tmask & (1u << f))) continue;
+#pragma unroll
+                for (int m = 0; m < R1; m++) x[f][m] = a.f[f][gb + m * q * g.gs_j];
+            }
+#pragma unroll
+            for (int f = 0; f < 3; f++) {
+                if (!(a.tmask & (1u << f))) continue;
+                dft<R1, -1>(x[f]);
+#pragma unroll
+                for (int k = 1; k < R1; k++) x[f][k] = twmul<-1>(x[f][k], ldtab<false>(tw + (k - 1) * q + b));
+                C *sp = sm + (size_t)f * g.region + off;
+#pragma unroll
+                for (int k = 0; k < R1; k++) sp[k * qs] = x[f][k];
+            }
+        }
+    } else
     for (int f = 0; f < nf; f++) {
         const int fid = field_id(a.tmask, f);
         const C *srcf = a.f[fid] + base;
