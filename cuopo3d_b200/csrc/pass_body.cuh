@@ -115,12 +115,10 @@ template <int BAR> __device__ __forceinline__ void tile_sync()
 // Index of the f-th field (in p, s, i order) selected by mask.
 __device__ __forceinline__ int field_id(unsigned mask, int f)
 {
-    for (int k = 0; k < 3; k++)
-        if (mask & (1u << k)) {
-            if (f == 0) return k;
-            f--;
-        }
-    return 0;
+    // the f-th set bit of a three-bit mask, without branches: clear the lowest set bit f times
+    mask = f > 0 ? mask & (mask - 1) : mask;
+    mask = f > 1 ? mask & (mask - 1) : mask;
+    return __ffs(mask) - 1;
 }
 
 // ---------------------------------------------------------------------------------
