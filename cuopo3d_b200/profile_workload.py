@@ -16,7 +16,7 @@ TUNED = {
     "fp32": {"t": dict(threads=128, tile=2048, r1=4), "x": dict(threads=128, tile=2048, r1=8),
              "y": dict(threads=128, tile=2048, r1=16)},
     "fp64": {"t": dict(threads=128, tile=1024, r1=4), "x": dict(threads=160, tile=1024, r1=8),
-             "y": dict(threads=160, tile=1024, r1=8)},
+             "y": dict(threads=288, tile=2048, r1=8)},
 }
 
 
