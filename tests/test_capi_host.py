@@ -103,7 +103,7 @@ def test_largest_volume_accepted():
 
 
 def test_zloop_step_counts():
-    """Step counts of the reference's float loop (Solver3D.cuh:949) for the BASELINE crystals."""
+    """Step counts of the reference's float loop (Solver3D.cuh:949) for the benchmark crystals."""
     for Lcr, nz, f32, expect in ((5000.0, 50, 1, 49), (20000.0, 100, 1, 100), (29000.0, 100, 1, 99)):
         _, sc = co.derive(co.make_config(Lcr=Lcr, nz=nz, zloop_f32=f32))
         assert sc["nsteps"] == expect
