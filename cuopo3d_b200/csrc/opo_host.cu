@@ -3,6 +3,7 @@
 // cavity round trip (captured as CUDA graphs), and the C-ABI of include/cuopo3d.h.
 
 #include "../../include/cuopo3d.h"
+#include "fft_gain.h"
 #include "opo_internal.h"
 #include "solver_internal.h"
 
@@ -654,6 +655,11 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     if ((rc = upload<C>(s, pc.allocs, tw, &pc.tw))) { free_pass(pc); return rc; }
     const bool phys = (p.flags & OPO_PHYSICS) != 0;
     const opo::AxisPlan &pl = pc.plan;
+    // FP32: every table of this plan carries the transform pair's gain compensation
+    const std::vector<double> comp = fp64 ? std::vector<double>() : opo::fp32_pair_compensation(pl, tw);
+    auto fix = [&](std::vector<cd> &t) {
+        if (!comp.empty()) opo::scale_table(t, comp);
+    };
     if (kind == kT) {
         // dispersion exp(i dz w (vinv + w b2/2)) exp(-alpha dz/2) / nt (Solver3D.cuh:153-169,
         // with the 1/nt of the inverse transform folded in); OPO_TOD adds w^3 b3/6 to the
@@ -668,6 +674,7 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
                 if (!phys) v *= std::exp(-0.5 * p.alpha[f] * p.dz);
                 tab[pos] = v * (q2scale / nt);
             }
+            fix(tab);
             if ((rc = upload<TT>(s, pc.allocs, tab, &pc.tab[0][f]))) { free_pass(pc); return rc; }
         }
         // GDD compensation exp(i w^2 GDD / 2) (Solver3D.cuh:261-277, 676) times the mirror
@@ -681,6 +688,7 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
                 const double wk = s->w[bin_of_position(pl, pos)];
                 tab[pos] = std::polar(1.0, 0.5 * wk * wk * p.gdd) * mirror / (double)nt;
             }
+            fix(tab);
             if ((rc = upload<TT>(s, pc.allocs, tab, &pc.tab[1][f]))) { free_pass(pc); return rc; }
         }
         if (p.eom_beta != 0) {
@@ -695,6 +703,10 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     } else {
         std::vector<cd> crys[3], free[3];
         diffraction_tables(p, kind == kX, pl, crys, free);
+        for (int f = 0; f < 3; f++) {
+            fix(crys[f]);
+            fix(free[f]);
+        }
         for (int f = 0; f < 3; f++)
             if ((rc = upload<TT>(s, pc.allocs, crys[f], &pc.tab[0][f])) ||
                 (rc = upload<TT>(s, pc.allocs, free[f], &pc.tab[1][f]))) {
@@ -769,7 +781,14 @@ template <typename C> int configure_plane(OpoSolver *s, int K, int threads, int 
         return rc;
     }
     std::vector<cd> crys[3], free[3];
+    // FP32: the same gain compensation as the separate x / y passes' tables
+    std::vector<double> comp;
+    if (!fp64) comp = opo::fp32_pair_compensation(pc.px, twx);
     diffraction_tables(p, true, pc.px, crys, free);
+    for (int f = 0; f < 3 && !comp.empty(); f++) {
+        opo::scale_table(crys[f], comp);
+        opo::scale_table(free[f], comp);
+    }
     for (int f = 0; f < 3; f++)
         if ((rc = upload<TT>(s, pc.allocs, crys[f], &pc.tabx[0][f])) ||
             (rc = upload<TT>(s, pc.allocs, free[f], &pc.tabx[1][f]))) {
@@ -777,6 +796,11 @@ template <typename C> int configure_plane(OpoSolver *s, int K, int threads, int 
             return rc;
         }
     diffraction_tables(p, false, pc.py, crys, free);
+    if (!fp64) comp = opo::fp32_pair_compensation(pc.py, twy);
+    for (int f = 0; f < 3 && !comp.empty(); f++) {
+        opo::scale_table(crys[f], comp);
+        opo::scale_table(free[f], comp);
+    }
     for (int f = 0; f < 3; f++)
         if ((rc = upload<TT>(s, pc.allocs, crys[f], &pc.taby[0][f])) ||
             (rc = upload<TT>(s, pc.allocs, free[f], &pc.taby[1][f]))) {

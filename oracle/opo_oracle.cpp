@@ -595,6 +595,7 @@ int or_setup(const OrPhys *in, OrParams *o, double *sc, double *t, double *w, do
     o->vinv[2] = 1 / v[2] - 1 / v[1];
     o->dk = dk;
     o->Rs = in->Rs; o->Ri = in->Ri; o->detuning = in->detuning;
+    o->resonant = in->resonant;
     o->gdd = in->gdd_gamma != 0 ? -(in->gdd_gamma) * b2[1] * in->Lcr : 0.0;  // Solver3D.cuh:676
     o->free_len = in->Lcr;  // Solver3D.cuh:989
     o->total_rt = in->total_rt;
@@ -722,8 +723,9 @@ int or_round_trips(OrParams *p, const double *w, const double *Api, double *Ap, 
             q.flags &= ~(unsigned)OR_ASIS_Q2;
             tAxisOp(&q, r.cache, F, r.gddTab, 6u);
         }
-        const cd ms = std::sqrt(p->Rs) * cpxExp(p->detuning);
-        const cd mi = std::sqrt(p->Ri) * cpxExp(p->detuning);
+        // only resonant fields meet a mirror (Solver3D.cuh:993-994)
+        const cd ms = (p->resonant & 2u) ? std::sqrt(p->Rs) * cpxExp(p->detuning) : cd(1, 0);
+        const cd mi = (p->resonant & 4u) ? std::sqrt(p->Ri) * cpxExp(p->detuning) : cd(1, 0);
 #pragma omp parallel for schedule(static)
         for (long long v = 0; v < (long long)V; v++) {
             F[1][v] = ms * F[1][v];

@@ -64,6 +64,7 @@ typedef struct {
     int total_rt;                /* round trips of the run (last one skips free space) */
     unsigned pol;                /* ZGP: bit f set = wave f (p, s, i) extraordinary   */
     double eom_beta, eom_fpm;    /* intracavity EOM (Cavity1D.cuh:75-84); beta 0: none */
+    unsigned resonant;           /* mirrors act on fields with bit f set (2 s, 4 i)  */
 } OrPhys;
 
 /* Everything the split-step needs, derived from OrPhys. */
@@ -82,6 +83,7 @@ typedef struct {
     int rt_index;       /* round trips done so far (in/out)      */
     double beta3[3];    /* third-order dispersion (OR_TOD)       */
     double eom_beta, eom_fpm, t_window;
+    unsigned resonant;
 } OrParams;
 
 /* Derived scalars, in this order (the harness dump uses the same names):

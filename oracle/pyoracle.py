@@ -56,6 +56,7 @@ class OrPhys(ctypes.Structure):
         ("total_rt", ctypes.c_int),
         ("pol", ctypes.c_uint),
         ("eom_beta", ctypes.c_double), ("eom_fpm", ctypes.c_double),
+        ("resonant", ctypes.c_uint),
     ]
 
 
@@ -75,6 +76,7 @@ class OrParams(ctypes.Structure):
         ("total_rt", ctypes.c_int), ("rt_index", ctypes.c_int),
         ("beta3", ctypes.c_double * 3),
         ("eom_beta", ctypes.c_double), ("eom_fpm", ctypes.c_double), ("t_window", ctypes.c_double),
+        ("resonant", ctypes.c_uint),
     ]
 
 
@@ -118,7 +120,7 @@ def make_phys(**kw):
              alpha=(-1.0, -1.0, -1.0), Lcav=-1.0, Rs=0.98, Ri=None, gdd_gamma=0.0,
              detuning=0.0, P=1.0, FWHM=2.0, w0=50.0, focal=None, pump_mode="focused-pulsed",
              t_window=0.0, flags=OR_DISPERSION | OR_DIFFRACTION, zloop_f32=0, n_steps=0,
-             total_rt=1, pol="eeo", eom_beta=0.0, eom_fpm=0.0)
+             total_rt=1, pol="eeo", eom_beta=0.0, eom_fpm=0.0, resonant=6)
     d.update(kw)
     if isinstance(d["pol"], str):
         d["pol"] = sum(1 << f for f, ch in enumerate(d["pol"]) if ch == "e")

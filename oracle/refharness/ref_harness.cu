@@ -250,6 +250,11 @@ static int run(const Args &a)
     real_t focal = argd(a, "focal", Lcr / 2);
     EFields<Crystal> *A = new EFields<Crystal>(lp, ls, li, P, w0, cr);
     A->resFields = std::make_tuple(false, true, true);
+    if (a.count("resonant")) {
+        // bit mask of resonant fields (1 pump, 2 signal, 4 idler), default signal + idler as main()
+        const int r = (int)argd(a, "resonant", 6);
+        A->resFields = std::make_tuple((r & 1) != 0, (r & 2) != 0, (r & 4) != 0);
+    }
     real_t twin = argd(a, "twin", 0);
     A->setTimeFreqVectors(twin > 0 ? twin : cav->trt);
     A->setPumpField(P, FWHM, w0, focal, args(a, "pump", "focused-pulsed"));

@@ -8,14 +8,15 @@ are not stored: they are regenerated from the recorded seed with the oracle's
 counter-based noise (identical IEEE operations everywhere), written to files and
 uploaded to the reference in place of its wall-clock-seeded noise.
 
-Run (GPU box):  python tests/golden/make_golden.py --out gpurun_out/golden
-then copy the .npz files into tests/golden/.
+Run on a machine with a B200:  python tests/golden/make_golden.py --out DIR [--only NAMES]
+then copy the .npz files from DIR into tests/golden/.
 """
 import argparse
 import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -59,6 +60,15 @@ CASES = [
           lp=0.532, ls=1.064, dQ=14e-6, P=1, FWHM=2, w0=50, focal=2500, twin=20,
           pump="focused-pulsed"),
      (1, "rel:1e-6"), "zero", [0, 16, 32, 48]),
+    # the benchmark workload: singly-resonant OPO at full size, 10 round trips of 100 steps;
+    # slices at the signal / idler centre (128), where the pump leaves the crystal after
+    # its group-delay walk-off in the pump frame, L (1/vp - 1/vi) = 16.4 ps (232), and
+    # between them (180)
+    ("c2_opo_fp64", "c2_fp64fix", (128, 128, 256),
+     dict(mode="opo", crystal="ppln", LX=800, LY=800, Lcr=20000, T=27, Lambda=6.97,
+          lp=0.532, ls=1.064, Rs=0.98, P=5, FWHM=2, w0=60, focal=10000, twin=40,
+          pump="focused-pulsed", alpha_p=2e-7, alpha_s=2e-7, alpha_i=2e-7, resonant=2),
+     (1, "rel:1e-6"), "zero", [128, 180, 232]),
 ]
 
 TIMING = [
@@ -97,8 +107,14 @@ def run_case(case, out_dir):
     name, binary, shape, args, (seed, sigma), idler, tsl = case
     nx, ny, nt = shape
     V = nx * ny * nt
-    tmp = os.path.join(out_dir, "tmp_" + name)
-    os.makedirs(tmp, exist_ok=True)
+    # the full fields the harness exchanges (hundreds of MB at 128 x 128 x 256) stay in a
+    # temporary directory; only the fixture goes to out_dir
+    with tempfile.TemporaryDirectory(prefix="golden_" + name + "_") as tmp:
+        run_case_in(name, binary, shape, args, seed, sigma, idler, tsl, V, tmp, out_dir)
+
+
+def run_case_in(name, binary, shape, args, seed, sigma, idler, tsl, V, tmp, out_dir):
+    nx, ny, nt = shape
     if isinstance(sigma, str):
         rel = float(sigma.split(":")[1])
         api = po.Setup(oracle_phys_for(args, shape)).api_complex()
@@ -113,6 +129,8 @@ def run_case(case, out_dir):
     cmd = [os.path.join(REF_DIR, "ref_" + binary)] + harness_args(a)
     t0 = time.time()
     proc = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    with open(os.path.join(out_dir, name + ".log"), "w") as f:
+        f.write(proc.stdout + proc.stderr)
     if proc.returncode != 0 or "RH_DONE" not in proc.stdout:
         raise RuntimeError(f"{name}: rc={proc.returncode}\n{proc.stdout[-2000:]}\n{proc.stderr[-2000:]}")
     if a["mode"] == "opo" and "criteria: passed" not in proc.stdout:
@@ -131,7 +149,9 @@ def run_case(case, out_dir):
                scalar_values=np.array(list(sc.values())), t=t, w=w, tidx=tidx,
                Api=fields["Api"][tidx], Ap=fields["Ap"][tidx], As=fields["As"][tidx],
                Ai=fields["Ai"][tidx],
-               norms=np.array([np.sum(np.abs(fields[k]) ** 2) for k in ("Ap", "As", "Ai")]))
+               norms=np.array([np.sum(np.abs(fields[k]) ** 2) for k in ("Ap", "As", "Ai")]),
+               # energy of every t-slice of each output field, [field][t]
+               tprof=np.array([np.sum(np.abs(fields[k]) ** 2, axis=(1, 2)) for k in ("Ap", "As", "Ai")]))
     np.savez_compressed(os.path.join(out_dir, name + ".npz"), **out)
     print(f"{name}: ok in {meta['seconds']:.1f}s nsteps={sc['nsteps']:.0f} "
           f"|As|^2={out['norms'][1]:.6e}", flush=True)
@@ -157,7 +177,7 @@ def run_timing(out_dir, steps, warmup):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", required=True, help="directory for the new .npz fixtures")
     ap.add_argument("--only", default="")
     ap.add_argument("--timing", action="store_true")
     ap.add_argument("--steps", type=int, default=3)

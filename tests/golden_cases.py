@@ -23,6 +23,8 @@ class Golden:
         self.t, self.w, self.tidx = z["t"], z["w"], z["tidx"]
         self.Api, self.Ap, self.As, self.Ai = z["Api"], z["Ap"], z["As"], z["Ai"]
         self.norms = z["norms"]
+        # energy of every t-slice of Ap, As, Ai (newer fixtures), else None
+        self.tprof = z["tprof"] if "tprof" in z.files else None
         nx, ny, nt = self.meta["shape"]
         self.nx, self.ny, self.nt = nx, ny, nt
         self.fp64 = bool(self.scalars["fp64"])
@@ -41,7 +43,12 @@ class Golden:
     def config_kwargs(self):
         """Keyword arguments shared by the oracle's OrPhys and the library's OpoConfig."""
         a = self.args
-        return dict(crystal=0 if a["crystal"] == "ppln" else 1, LX=a["LX"], LY=a["LY"],
+        extra = {}
+        if "alpha_p" in a:
+            extra["alpha"] = (a["alpha_p"], a["alpha_s"], a["alpha_i"])
+        if "resonant" in a:
+            extra["resonant"] = a["resonant"]
+        return dict(extra, crystal=0 if a["crystal"] == "ppln" else 1, LX=a["LX"], LY=a["LY"],
                     Lcr=a["Lcr"], T=a["T"], Lambda=a["Lambda"], lp=a["lp"], ls=a["ls"],
                     nx=self.nx, ny=self.ny, nt=self.nt, nz=self.nz, dQ=a.get("dQ", -1.0),
                     Lcav=a.get("Lcav", 4 * a["Lcr"]), Rs=a.get("Rs", 0.98),

@@ -170,3 +170,45 @@ def test_incompatible_grid_rejected():
     b = make_batch()
     with pytest.raises(co.OpoError):
         b.add(cfg_of(dict(nx=12, ny=12, nt=24, P=10.0, w0=40.0)))  # 12 has no radix-8 first stage
+
+
+def c4_instances(n=9, seed=2024):
+    """Instances over the batched form's grid set, N x N x NT with N in {32, 64, 128} and
+    NT in {64, 128, 256} (every pair once), P log-uniform 0.5-20 W, waist U[30, 100] um,
+    detuning U[-pi, pi]; a 2 mm crystal over a 1600 um window in 4 slices keeps the
+    oracle's run to seconds (the 128 x 128 x 256 instances dominate)."""
+    rng = np.random.default_rng(seed)
+    pairs = [(N, NT) for N in (32, 64, 128) for NT in (64, 128, 256)][:n]
+    out = []
+    for N, NT in pairs:
+        out.append(dict(nx=N, ny=N, nt=NT, nz=4, LX=1600.0, LY=1600.0, Lcr=2000.0, t_window=40.0,
+                        P=float(np.exp(rng.uniform(np.log(0.5), np.log(20.0)))), w0=float(rng.uniform(30, 100)),
+                        detuning=float(rng.uniform(-np.pi, np.pi)), FWHM=2.0, focal=1000.0, Rs=0.98,
+                        alpha=(2e-7, 2e-7, 2e-7), pump_mode="focused-pulsed", total_rt=2))
+    return out
+
+
+@pytest.mark.parametrize("precision,tol", [(co.FP64, 1e-10), (co.FP32, 1e-5)])
+def test_batch_c4_grid_set_vs_oracle(precision, tol):
+    """Every grid of the batched form's set in one batch (FP64: the plain form, FP32: the
+    precision form) against the FP64 oracle on the same inputs, two round trips."""
+    insts = c4_instances()
+    tuning = TUNING if precision == co.FP64 else {"t": dict(threads=128, tile=2048, r1=8),
+                                                  "x": dict(threads=128, tile=2048, r1=8),
+                                                  "y": dict(threads=128, tile=2048, r1=16)}
+    b = co.Batch(precision, len(insts), 16 << 30, tuning=tuning)
+    slots = []
+    for k, kw in enumerate(insts):
+        cfg = co.make_config(precision=precision, **kw)
+        s = b.add(cfg)
+        b.init_fields(s, cfg, 300 + k, 0.01)
+        slots.append(s)
+    b.run_round_trips(2)
+    for k, kw in enumerate(insts):
+        got = [b.get_field(slots[k], w) for w in (co.FIELD_AP, co.FIELD_AS, co.FIELD_AI)]
+        st = po.Setup(po.make_phys(**kw))
+        api = st.api_complex()
+        s0 = co.noise(300 + k, 0.01, api.size).reshape(api.shape)
+        ref = po.round_trips(st, api, api, s0, np.zeros_like(s0), 2)
+        for name, a, c in zip(("Ap", "As", "Ai"), got, ref):
+            assert rel_l2(a, c) < tol, (kw["nx"], kw["nt"], name, rel_l2(a, c))

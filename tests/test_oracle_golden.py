@@ -8,6 +8,15 @@ from golden_cases import Golden, fixture_names, rel_l2
 from oracle import pyoracle as po
 
 NAMES = fixture_names()
+# Fixtures whose split-step run takes the oracle more than a few seconds on the host
+# cores (the 128x128x256, 10-round-trip benchmark case: ~4e9 voxel-steps) get their
+# scalars, grids and pump checked here; their output fields are checked against the
+# FP64 CUDA path in tests/test_gpu_parity.py.
+MAX_ORACLE_VOXEL_STEPS = 2e8
+
+
+def heavy(g):
+    return g.nx * g.ny * g.nt * int(g.scalars["nsteps"]) * max(1, g.nrt) > MAX_ORACLE_VOXEL_STEPS
 
 
 def oracle_run(g):
@@ -18,6 +27,8 @@ def oracle_run(g):
     st = po.Setup(ph)
     s0, i0 = g.initial_fields(po.noise)
     api = st.api_complex()
+    if heavy(g):
+        return st, api, None
     if g.mode == "single":
         out = po.single_pass(st, api, s0, i0)
     else:
@@ -61,7 +72,10 @@ def test_pump_matches_reference(case):
 
 def test_fields_match_reference(case):
     """Output fields of the split-step (single pass or cavity round trips)."""
-    g, (_, _, (ap, as_, ai)) = case
+    g, (_, _, out) = case
+    if out is None:
+        pytest.skip("fields of this fixture are checked against the FP64 CUDA path (GPU tests)")
+    ap, as_, ai = out
     if g.fp64:
         tol = 1e-10
     else:
