@@ -7,18 +7,30 @@ Workload: the singly-resonant OPO at full size -- PPLN 20 mm, 128 x 128 x 256 gr
 mismatch on, absorption 0.002/cm, signal mirror R = 0.98, detuning 0, 60 um / 5 W / 2 ps
 Gaussian pump, noise-seeded signal, FP64 fields.  One step = one cavity round trip
 (100 z-steps of 4,194,304 voxels).  The metric is voxel-steps/s (one voxel of all three
-fields advanced through one full split step); `value` is device-timed with inputs
-resident; `e2e` runs every step through the C-ABI from pinned host buffers (inputs up, one
-round trip, signal down), two solvers alternating so that host copies overlap compute.
+fields advanced through one full split step).
+  value      device-timed (CUDA events on the solver's stream), inputs resident in HBM
+  e2e        through the C-ABI with host buffers, one solver: every step uploads its
+             three input fields from pinned host memory, runs one round trip and reads
+             its three output fields back to pinned host memory, all inside the timed
+             region (e2e_pipelined: two solvers alternate so one's copies overlap the
+             other's round trip, the way a sweep drives the library)
+Extra legs on rank 0 (N = 1): the FP32 precision form, the batched form (64 uneven
+instances, FP32 and FP64, kernel configuration tuned for the mix), the served form (a
+Poisson stream with 50-500 round trips per request, FP32 and FP64, p50/p99 latency and
+the FP32 results' error against FP64), the FP32 error per round trip on the batched
+form's grids, and the FP64 CPU oracle as the reported CPU baseline.
 
 Multi-GPU: every rank runs its own independent instance (weak scaling, no collective on
-the data path); value = all ranks' voxel-steps / the slowest rank's time.
+the data path); value = all ranks' voxel-steps / the slowest rank's time.  The batched
+mix (64 instances per rank) is sharded over the ranks by longest-processing-time first.
 
 `--impl reference` times the reference's own cuFFT pipeline (its headers compiled by
 oracle/refharness into oracle/_ref/, unmodified code path, FP32 as shipped) on the same
-GPU; without that build it times the FP64 CPU oracle on the host cores instead.
+GPU for --steps round trips after --warmup; without that build it times the FP64 CPU
+oracle on the host cores instead.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -39,8 +51,12 @@ WORKLOAD = dict(nx=128, ny=128, nt=256, nz=100, LX=800.0, LY=800.0, Lcr=20000.0,
                 detuning=0.0, total_rt=200, resonant=2)
 WORKLOAD_NAME = ("singly-resonant OPO, PPLN 20 mm, 128x128x256 over 800 um / 40 ps, 100 z-steps, "
                  "5 W 60 um 2 ps pump, R=0.98, one cavity round trip per step")
+V = 128 * 128 * 256
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM = 6650.0
+# batched and served instances: 20 mm PPLN, 100 slices, 800 um / 40 ps windows
+FORM_BASE = dict(nz=100, LX=800.0, LY=800.0, Lcr=20000.0, t_window=40.0, FWHM=2.0, focal=10000.0, Rs=0.98,
+                 alpha=(2e-7, 2e-7, 2e-7), zloop_f32=1, pump_mode="focused-pulsed")
 
 
 def hbm_peak():
@@ -184,13 +200,94 @@ def time_device(sim, steps, world, tag):
     return max_over_ranks(e0.elapsed_time(e1), world)
 
 
-def run_ours(args):
+class HostIO:
+    """Pinned host buffers of one step's inputs (Api, As, Ai) and outputs (Ap, As, Ai),
+    complex128, moved through the C-ABI (opo_set_field / opo_get_field with host memory)."""
+
+    def __init__(self, co, api, s0):
+        import torch
+        self.co = co
+        self.inp = [torch.from_numpy(np.ascontiguousarray(a, dtype=np.complex128).reshape(-1)).pin_memory()
+                    for a in (api, s0, np.zeros_like(s0))]
+        self.out = [torch.empty(V, dtype=torch.complex128).pin_memory() for _ in range(3)]
+
+    def h2d_bytes(self):
+        return sum(t.numel() * 16 for t in self.inp)
+
+    def d2h_bytes(self):
+        return sum(t.numel() * 16 for t in self.out)
+
+    def put(self, sim):
+        co = self.co
+        for which, t in zip((co.FIELD_API, co.FIELD_AS, co.FIELD_AI), self.inp):
+            rc = co.lib().opo_set_field(sim.handle, which, ctypes.c_void_p(t.data_ptr()), co.MEM_HOST, co.FP64)
+            assert rc == 0, rc
+
+    def get(self, sim, out=None):
+        co = self.co
+        for which, t in zip((co.FIELD_AP, co.FIELD_AS, co.FIELD_AI), out or self.out):
+            rc = co.lib().opo_get_field(sim.handle, which, ctypes.c_void_p(t.data_ptr()), co.MEM_HOST, co.FP64)
+            assert rc == 0, rc
+
+
+def e2e_single(co, sim, io, steps, world, nsteps):
+    """One solver: every step uploads its inputs, runs one round trip, reads its outputs
+    (opo_get_field into host memory waits for the solver's stream)."""
+    io.put(sim)
+    sim.run_round_trips(1)
+    io.get(sim)
+    barrier_sync(world)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        io.put(sim)
+        sim.run_round_trips(1)
+        io.get(sim)
+    barrier_sync(world)
+    dt = max_over_ranks(time.perf_counter() - t0, world)
+    return sum_over_ranks(float(V) * nsteps * steps, world) / dt
+
+
+def e2e_pipelined(co, params, sim, io, steps, world, nsteps):
+    """Two solvers alternate (step k on solver k % 2): step k+1's uploads and round trip
+    are enqueued before step k's outputs are read, so one solver's host copies run on the
+    copy engines while the other's round trip runs on the SMs."""
     import torch
+    _, w = co.time_freq(params.nt, params.t_window)
+    sim2 = co.Simulation(params, w)
+    sim2.autotune()  # cached: the same configuration as sim
+    sims = (sim, sim2)
+    outs = [io.out, [torch.empty(V, dtype=torch.complex128).pin_memory() for _ in range(3)]]
+
+    def enqueue(k):
+        io.put(sims[k % 2])
+        sims[k % 2].run_round_trips(1)
+
+    def collect(k):
+        io.get(sims[k % 2], outs[k % 2])
+
+    enqueue(0)
+    enqueue(1)
+    collect(0)
+    collect(1)
+    barrier_sync(world)
+    t0 = time.perf_counter()
+    enqueue(0)
+    for k in range(steps):
+        if k + 1 < steps:
+            enqueue(k + 1)
+        collect(k)
+    barrier_sync(world)
+    dt = max_over_ranks(time.perf_counter() - t0, world)
+    sim2.close()
+    return sum_over_ranks(float(V) * nsteps * steps, world) / dt
+
+
+def run_ours(args):
     import cuopo3d_b200 as co
     rank, world, local = dist_setup(args.gpus)
-    V = 128 * 128 * 256
     out = {}
     hbm, hbm_kind = hbm_peak()
+    e2e_steps = max(4, args.steps // 2)
     for prec, tag, bpv in ((co.FP64, "fp64", 96), (co.FP32, "fp32", 48)):
         cfg, params, sim, api, s0 = make_instance(co, prec, seed=1 + rank)
         nsteps = params.n_steps
@@ -218,56 +315,19 @@ def run_ours(args):
                 avg_us = tot / n * 1e3
                 passes[k] = {"avg_us": round(avg_us, 2), "launches": n,
                              "alg_GBps": round(V * bpv / (avg_us * 1e-6) / 1e9, 1)}
-        # End to end through the C-ABI: every step uploads its three input fields from pinned
-        # host memory, runs one round trip and reads its signal back to pinned host memory.
-        # Two solvers alternate (step k on solver k % 2): step k+1's uploads and round trip
-        # are enqueued before step k's result is read, so one solver's host copies run on
-        # the copy engines while the other's round trip runs on the SMs.
-        pin = {k: torch.from_numpy(np.ascontiguousarray(a, dtype=np.complex128).reshape(-1)).pin_memory()
-               for k, a in (("api", api), ("s", s0), ("i", np.zeros_like(s0)))}
-        _, w2 = co.time_freq(cfg.nt, params.t_window)
-        sim2 = co.Simulation(params, w2)
-        sim2.autotune()  # cached: the same configuration as sim
-        upload(co, sim2, api, s0)
-        sims = (sim, sim2)
-        res = [torch.empty(V, dtype=torch.complex128).pin_memory() for _ in sims]
-        lib = co.lib()
-        import ctypes
-
-        def enqueue(k):
-            h = sims[k % 2].handle
-            for which, t in ((co.FIELD_API, pin["api"]), (co.FIELD_AS, pin["s"]), (co.FIELD_AI, pin["i"])):
-                rc = lib.opo_set_field(h, which, ctypes.c_void_p(t.data_ptr()), co.MEM_HOST, co.FP64)
-                assert rc == 0
-            sims[k % 2].run_round_trips(1)
-
-        def collect(k):
-            rc = lib.opo_get_field(sims[k % 2].handle, co.FIELD_AS, ctypes.c_void_p(res[k % 2].data_ptr()),
-                                   co.MEM_HOST, co.FP64)
-            assert rc == 0
-
-        enqueue(0)
-        enqueue(1)
-        collect(0)
-        collect(1)
-        e2e_steps = max(4, args.steps // 2)
-        barrier_sync(world)
-        t0 = time.perf_counter()
-        enqueue(0)
-        for k in range(e2e_steps):
-            if k + 1 < e2e_steps:
-                enqueue(k + 1)
-            collect(k)
-        barrier_sync(world)
-        e2e_s = max_over_ranks(time.perf_counter() - t0, world)
-        e2e_value = sum_over_ranks(float(V) * nsteps * e2e_steps, world) / e2e_s
-        sim2.close()
+        io = HostIO(co, api, s0)
+        e2e = e2e_single(co, sim, io, e2e_steps, world, nsteps)
+        e2e_pipe = e2e_pipelined(co, params, sim, io, e2e_steps, world, nsteps)
         out[tag] = dict(value=value, ms_per_step=ms / args.steps, launches=launches, passes=passes,
-                        tuning=sim.tuning,
-                        clocks=clk.summary(), nsteps=nsteps,
-                        e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=3 * V * 16,
-                                 d2h_bytes_per_step=V * 16))
+                        tuning=sim.tuning, clocks=clk.summary(), nsteps=nsteps,
+                        e2e=dict(value=e2e, unit=UNIT, h2d_bytes_per_step=io.h2d_bytes(),
+                                 d2h_bytes_per_step=io.d2h_bytes(), solvers=1, steps=e2e_steps),
+                        e2e_pipelined=dict(value=e2e_pipe, unit=UNIT, h2d_bytes_per_step=io.h2d_bytes(),
+                                           d2h_bytes_per_step=io.d2h_bytes(), solvers=2, steps=e2e_steps))
         sim.close()
+    legs = {}
+    if world > 1 and not args.no_forms:
+        legs["batched_sharded"] = batched_sharded_leg(co, rank, world, args.batched_instances)
     if rank == 0:
         main = out["fp64"]
         t = main["passes"].get("t")
@@ -288,6 +348,7 @@ def run_ours(args):
                        "global_batch": world, "parallelism": f"independent instances x{world}",
                        "l2": "inputs larger than L2 (FP64 state 201 MB + pump 67 MB > 126 MB)"},
             "e2e": main["e2e"],
+            "e2e_pipelined": main["e2e_pipelined"],
             "gpu_launches": main["launches"],
             "clocks": main["clocks"],
             "roofline": {"bound": "hbm", "kernel": "tpass_kernel<double2> (RK4 x2 + t-axis FFT pair)",
@@ -302,17 +363,16 @@ def run_ours(args):
                                    "alg_flops_per_launch": flops_t},
             "passes_fp64": main["passes"],
             "tuning_fp64": main["tuning"],
-            "fp32": {"value": out["fp32"]["value"], "ms_per_step": out["fp32"]["ms_per_step"],
-                     "passes": out["fp32"]["passes"], "e2e": out["fp32"]["e2e"],
-                     "clocks": out["fp32"]["clocks"], "tuning": out["fp32"]["tuning"]},
+            "fp32": {k: out["fp32"][k] for k in ("value", "ms_per_step", "passes", "e2e", "e2e_pipelined",
+                                                  "clocks", "tuning")},
         }
-        if not args.no_forms:
-            tun = out["fp32"]["tuning"]
-            line["batched"] = batched_leg(co, tun, n_inst=args.batched_instances)
-            # arrival rate at ~85 % of capacity: throughput / mean work of a request
-            mean_vox = (64 * 64 * 128 + 128 * 128 * 256 + 96 * 96 * 192) / 3.0
-            rate = 0.85 * line["batched"]["value"] / (mean_vox * 100 * 15)
-            line["served"] = served_leg(co, tun, rate, n_req=args.served_requests)
+        line.update(legs)
+        if world == 1 and not args.no_forms:
+            line["batched"] = batched_leg(co, co.FP32, args.batched_instances)
+            line["batched_fp64"] = batched_leg(co, co.FP64, args.batched_instances)
+            line["served"] = served_leg(co, co.FP32, args.served_requests, line["batched"]["value"])
+            line["served_fp64"] = served_leg(co, co.FP64, args.served_requests_fp64, line["batched_fp64"]["value"])
+            line["precision"] = precision_leg(co)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
@@ -321,25 +381,29 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def batched_leg(co, tuning, n_inst=64, warm=1, steps=3, seed=2024):
-    """Batched form: n_inst instances with grids drawn from N in {32, 64, 128} and
-    NT in {64, 128, 256}, P log-uniform 0.5-20 W, waist U[30, 100] um, detuning U[-pi, pi],
-    20 mm PPLN, 100 slices, FP32; one persistent launch per pass for all of them."""
-    import torch
+def c4_mix(n_inst, seed=2024, precision=None):
+    """The batched form's instance mix: N x N x NT with N in {32, 64, 128} and NT in
+    {64, 128, 256}, P log-uniform 0.5-20 W, waist U[30, 100] um, detuning U[-pi, pi],
+    200 round trips each; list of make_config keyword dicts."""
     rng = np.random.default_rng(seed)
-    b = co.Batch(co.FP32, n_inst, 150 << 30, tuning=tuning)
-    vox = 0
-    for k in range(n_inst):
+    out = []
+    for _ in range(n_inst):
         N = int(rng.choice([32, 64, 128]))
         NT = int(rng.choice([64, 128, 256]))
-        cfg = co.make_config(nx=N, ny=N, nt=NT, nz=100, LX=800.0, LY=800.0, Lcr=20000.0, t_window=40.0,
-                             P=float(np.exp(rng.uniform(np.log(0.5), np.log(20.0)))),
-                             w0=float(rng.uniform(30, 100)), detuning=float(rng.uniform(-np.pi, np.pi)),
-                             FWHM=2.0, focal=10000.0, Rs=0.98, alpha=(2e-7, 2e-7, 2e-7), zloop_f32=1,
-                             pump_mode="focused-pulsed", total_rt=200, precision=co.FP32)
+        out.append(dict(FORM_BASE, nx=N, ny=N, nt=NT, P=float(np.exp(rng.uniform(np.log(0.5), np.log(20.0)))),
+                        w0=float(rng.uniform(30, 100)), detuning=float(rng.uniform(-np.pi, np.pi)), total_rt=200))
+    return out
+
+
+def run_batch(co, precision, kws, tuning, seeds, warm=1, steps=3):
+    """Device time per batched round trip (ms) of the instances kws; kernel launches per
+    round trip."""
+    import torch
+    b = co.Batch(precision, len(kws), 150 << 30, tuning=tuning)
+    for kw, seed in zip(kws, seeds):
+        cfg = co.make_config(precision=precision, **kw)
         slot = b.add(cfg)
-        b.init_fields(slot, cfg, 1000 + k, 1e-3)
-        vox += N * N * NT
+        b.init_fields(slot, cfg, seed, 1e-3)
     b.run_round_trips(warm)
     b.synchronize()
     stream = torch.cuda.ExternalStream(b.stream)
@@ -352,37 +416,118 @@ def batched_leg(co, tuning, n_inst=64, warm=1, steps=3, seed=2024):
     ms = e0.elapsed_time(e1)
     launches = b.stats()["launches"] - l0
     b.close()
-    return {"value": vox * 100.0 * steps / (ms * 1e-3), "unit": UNIT, "instances": n_inst,
-            "voxels": vox, "round_trips_timed": steps, "ms_per_round_trip": ms / steps,
-            "launches_per_round_trip": launches / steps, "precision": "fp32",
-            "workload": f"{n_inst} instances, N in {{32,64,128}}, NT in {{64,128,256}}, 20 mm PPLN, 100 slices"}
+    return ms / steps, launches / steps
 
 
-def served_leg(co, tuning, rate_per_s, n_req=40, seed=7):
-    """Served form, bounded sample of the request stream: n_req Poisson arrivals at
-    rate_per_s, grids from {64^2x128, 128^2x256, 96^2x192}, P log-uniform 0.5-20 W,
-    waist U[30, 100] um, 5-25 round trips (retired early when the signal power changes by
-    less than 1e-6 over a round trip), 150 GB budget, FP32."""
+def batched_leg(co, precision, n_inst=64, steps=3):
+    """Batched form: n_inst instances of the C4 mix in one persistent launch per pass,
+    round trips replayed as CUDA graphs, kernel configuration tuned for this mix
+    (cuopo3d_b200.tuning.tune_batch)."""
+    from cuopo3d_b200.tuning import tune_batch
+    kws = c4_mix(n_inst)
+    seeds = [1000 + k for k in range(n_inst)]
+    cfgs = [co.make_config(precision=precision, **kw) for kw in kws]
+    t0 = time.perf_counter()
+    tuning, timed = tune_batch(precision, cfgs, 150 << 30, seeds)
+    tune_s = time.perf_counter() - t0
+    ms, launches = run_batch(co, precision, kws, tuning, seeds, steps=steps)
+    vox = sum(kw["nx"] * kw["ny"] * kw["nt"] for kw in kws)
+    return {"value": vox * 100.0 / (ms * 1e-3), "unit": UNIT, "instances": n_inst, "voxels": vox,
+            "round_trips_timed": steps, "ms_per_round_trip": ms, "launches_per_round_trip": launches,
+            "precision": "fp32" if precision == co.FP32 else "fp64", "tuning": tuning,
+            "tuning_candidates": [[t, s] for t, s in timed], "tuning_s": round(tune_s, 1),
+            "workload": f"{n_inst} instances, N in {{32,64,128}}, NT in {{64,128,256}}, P 0.5-20 W, "
+                        "w0 30-100 um, detuning U[-pi,pi], 20 mm PPLN, 100 slices"}
+
+
+def batched_sharded_leg(co, rank, world, per_rank=64, steps=3):
+    """The C4 mix with per_rank x world instances, sharded over the ranks by
+    longest-processing-time first (cost = voxels); every rank runs its share as one
+    batch; value = all instances' voxel-steps / the slowest rank's device time."""
+    from cuopo3d_b200 import shard
+    kws = c4_mix(per_rank * world, seed=4048)
+    costs = [kw["nx"] * kw["ny"] * kw["nt"] for kw in kws]
+    mine = shard.local_indices(costs, rank, world)
+    tuning = {"t": dict(threads=128, tile=2048, r1=8), "x": dict(threads=128, tile=2048, r1=8),
+              "y": dict(threads=128, tile=2048, r1=16)}
+    barrier_sync(world)
+    ms, _ = run_batch(co, co.FP32, [kws[k] for k in mine], tuning, [1000 + k for k in mine], steps=steps)
+    slowest = max_over_ranks(ms, world)
+    vox = sum(costs)
+    return {"value": vox * 100.0 / (slowest * 1e-3), "unit": UNIT, "instances": len(kws), "ranks": world,
+            "ms_per_round_trip_slowest_rank": slowest, "precision": "fp32", "sharding": "LPT by voxels"}
+
+
+def c5_requests(co, precision, n_req, rate_per_s, seed=7):
+    """n_req Poisson arrivals at rate_per_s, grids from {64^2x128, 128^2x256, 96^2x192},
+    P log-uniform 0.5-20 W, waist U[30, 100] um, 50-500 round trips, retired early when the
+    signal power changes by less than 1e-6 over a round trip."""
     rng = np.random.default_rng(seed)
     grids = [(64, 128), (128, 256), (96, 192)]
-    reqs, t = [], 0.0
+    reqs, kws, t = [], [], 0.0
     for k in range(n_req):
         t += float(rng.exponential(1.0 / rate_per_s))
         N, NT = grids[int(rng.integers(0, 3))]
-        cfg = co.make_config(nx=N, ny=N, nt=NT, nz=100, LX=800.0, LY=800.0, Lcr=20000.0, t_window=40.0,
-                             P=float(np.exp(rng.uniform(np.log(0.5), np.log(20.0)))),
-                             w0=float(rng.uniform(30, 100)), FWHM=2.0, focal=10000.0, Rs=0.98,
-                             alpha=(2e-7, 2e-7, 2e-7), zloop_f32=1, pump_mode="focused-pulsed",
-                             total_rt=int(rng.integers(5, 26)), precision=co.FP32)
-        reqs.append(dict(cfg=cfg, arrival_s=t, seed=5000 + k, noise_sigma=1e-3, tol=1e-6))
-    res, st = co.serve(reqs, co.FP32, capacity=1024, hbm_budget=150 << 30, realtime=True, tuning=tuning)
-    ok = sum(1 for r in res if r["status"] == co.OPO_OK)
-    return {"p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
-            "value": st["voxel_steps_per_s"], "unit": UNIT, "requests": n_req, "completed": ok,
-            "arrival_rate_per_s": rate_per_s, "wall_s": st["wall_s"], "max_resident": st["max_resident"],
-            "precision": "fp32",
-            "workload": "Poisson stream, grids {64^2x128, 128^2x256, 96^2x192}, 5-25 round trips, "
-                        "early retirement at |dPs/Ps| < 1e-6, 150 GB budget"}
+        kw = dict(FORM_BASE, nx=N, ny=N, nt=NT, P=float(np.exp(rng.uniform(np.log(0.5), np.log(20.0)))),
+                  w0=float(rng.uniform(30, 100)), total_rt=int(rng.integers(50, 501)))
+        kws.append(kw)
+        reqs.append(dict(cfg=co.make_config(precision=precision, **kw), arrival_s=t, seed=5000 + k,
+                         noise_sigma=1e-3, tol=1e-6))
+    return reqs, kws
+
+
+def served_leg(co, precision, n_req, batched_value, error_sample=2):
+    """Served form, a bounded sample of the request stream: n_req requests of the C5
+    distribution arriving at ~85 % of the batched throughput's capacity, 150 GB budget,
+    kernel configuration tuned for the request grids.  For FP32, the field and output-power
+    error of the error_sample shortest requests against FP64 (the same request run alone in
+    each precision; a served result equals its standalone run bit for bit)."""
+    from cuopo3d_b200.precision import error_of_request
+    from cuopo3d_b200.tuning import tune_batch
+    mean_vox = (64 * 64 * 128 + 128 * 128 * 256 + 96 * 96 * 192) / 3.0
+    rate = 0.85 * batched_value / (mean_vox * 100 * 275)  # mean request: 275 round trips
+    reqs, kws = c5_requests(co, precision, n_req, rate)
+    mix = [co.make_config(precision=precision, **dict(FORM_BASE, nx=N, ny=N, nt=NT, P=5.0, w0=60.0))
+           for N, NT in ((64, 128), (128, 256), (96, 192)) for _ in range(2)]
+    tuning, _ = tune_batch(precision, mix, 150 << 30)
+    res, st = co.serve(reqs, precision, capacity=1024, hbm_budget=150 << 30, realtime=True, tuning=tuning)
+    ok = [r for r in res if r["status"] == co.OPO_OK]
+    leg = {"p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
+           "value": st["voxel_steps_per_s"], "unit": UNIT, "requests": n_req, "completed": len(ok),
+           "arrival_rate_per_s": rate, "wall_s": st["wall_s"], "max_resident": st["max_resident"],
+           "round_trips_mean": float(np.mean([r["round_trips"] for r in res])),
+           "retired_steady": sum(1 for r, q in zip(res, kws) if r["status"] == co.OPO_OK and
+                                 r["round_trips"] < q["total_rt"]),
+           "precision": "fp32" if precision == co.FP32 else "fp64", "tuning": tuning,
+           "workload": f"{n_req} Poisson requests (a sample of the 2000-request stream), grids "
+                       "{64^2x128, 128^2x256, 96^2x192}, P 0.5-20 W, w0 30-100 um, 50-500 round trips, "
+                       "early retirement at |dPs/Ps| < 1e-6, 150 GB budget"}
+    if precision == co.FP32 and error_sample:
+        order = sorted(range(n_req), key=lambda k: res[k]["round_trips"] * kws[k]["nx"] ** 2 * kws[k]["nt"])
+        # the batch kernels run a warp-specialised CTA size as its consumer size
+        solo = {k: dict(v, threads={160: 128, 288: 256}.get(v["threads"], v["threads"])) for k, v in tuning.items()}
+        errs = []
+        for k in order[:error_sample]:
+            kw = dict(kws[k])
+            e = error_of_request(kw, 5000 + k, 1e-3, res[k]["round_trips"], tuning32=solo)
+            e["grid"] = [kw["nx"], kw["ny"], kw["nt"]]
+            errs.append(e)
+        leg["error_vs_fp64"] = errs
+    return leg
+
+
+def precision_leg(co, checkpoints=(1, 10, 50, 200)):
+    """FP32 against FP64 per round trip on grids of the batched form (N^2 x NT), the
+    bench workload's physics: relative L2 field error and output-power error."""
+    from cuopo3d_b200.precision import error_vs_round_trip
+    out = []
+    for N, NT in ((32, 64), (64, 128), (128, 256)):
+        kw = dict(WORKLOAD, nx=N, ny=N, nt=NT)
+        for r in error_vs_round_trip(kw, list(checkpoints)):
+            r["grid"] = [N, N, NT]
+            out.append(r)
+    return {"reference": "the FP64 plain form (<= 1e-10 from the FP64 oracle and the reference's FP64 build)",
+            "points": out}
 
 
 def cpu_baseline(z_steps=10):
@@ -400,7 +545,6 @@ def cpu_baseline(z_steps=10):
     t0 = time.perf_counter()
     po.single_pass(st, api, s0, np.zeros_like(s0))
     dt = time.perf_counter() - t0
-    V = 128 * 128 * 256
     return {"value": V * z_steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{z_steps} split steps (RK4 x2, dispersion, diffraction) of the 128x128x256 "
                       f"grid in FP64, {dt:.1f} s"}
@@ -408,19 +552,17 @@ def cpu_baseline(z_steps=10):
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     binary = os.path.join(ROOT, "oracle", "_ref", "ref_c2_fp32asis")
-    steps = max(1, min(args.steps, 5))
-    warm = max(1, min(args.warmup, 1))
+    steps, warm = max(1, args.steps), max(0, args.warmup)
     if os.path.exists(binary):
         a = dict(mode="time_opo", crystal="ppln", LX=800, LY=800, Lcr=20000, T=27, Lambda=6.97,
                  lp=0.532, ls=1.064, Rs=0.98, gdd=0.0, P=5, FWHM=2, w0=60, focal=10000, twin=40,
-                 pump="focused-pulsed", alpha_p=2e-7, alpha_s=2e-7, alpha_i=2e-7, steps=steps,
+                 pump="focused-pulsed", alpha_p=2e-7, alpha_s=2e-7, alpha_i=2e-7, resonant=2, steps=steps,
                  warmup=warm)
         cmd = [binary] + [f"{k}={v}" for k, v in a.items()]
-        p = subprocess.run(cmd, capture_output=True, text=True, timeout=1200)
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=1700)
         rec = None
         for ln in p.stdout.splitlines():
             if ln.startswith("{\"rh_time_opo\""):
@@ -452,17 +594,56 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# Pinned kernel configurations of the bench workload (the autotuner's choices on a B200),
+# for profiling runs whose launch order must not depend on a timing-based choice.
+PINNED_TUNING = {
+    "fp32": {"t": dict(threads=128, tile=2048, r1=8), "x": dict(threads=128, tile=2048, r1=8),
+             "y": dict(threads=128, tile=2048, r1=16)},
+    "fp64": {"t": dict(threads=128, tile=1024, r1=4), "x": dict(threads=160, tile=1024, r1=8),
+             "y": dict(threads=288, tile=2048, r1=8)},
+}
+
+
+def profile_workload(precision, round_trips, plane=0):
+    """The bench workload with a pinned kernel configuration and no timing, for profilers:
+    4 field-conversion kernels (fields uploaded from FP64 host arrays), then per round trip
+    n t-passes, n x- and y-passes, the closing t-pass and the free-space x'/y' passes
+    (3n + 3 launches; with plane = K the x and y passes are one plane pass: 2n + 2)."""
+    import cuopo3d_b200 as co
+    prec = co.FP64 if precision == "fp64" else co.FP32
+    cfg = co.make_config(precision=prec, **WORKLOAD)
+    params, _ = co.derive(cfg)
+    _, w = co.time_freq(cfg.nt, params.t_window)
+    sim = co.Simulation(params, w)
+    sim.set_tuning(PINNED_TUNING[precision])
+    sim.set_plane_pass(plane)
+    api = co.pump_field(cfg)
+    s0 = co.noise(1, 1e-6 * float(np.max(np.abs(api))), api.size).reshape(api.shape)
+    upload(co, sim, api, s0)
+    sim.run_round_trips(round_trips)
+    sim.synchronize()
+    print("ok", sim.kernel_launches, sim.tuning)
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--profile-passes", choices=("fp32", "fp64"),
+                    help="run the workload with the pinned kernel configuration, untimed (for profilers)")
+    ap.add_argument("--round-trips", type=int, default=1, help="round trips of --profile-passes")
+    ap.add_argument("--plane", type=int, default=0, help="--profile-passes: plane-pass cluster size (0: x and y)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-forms", action="store_true", help="skip the batched and served legs")
-    ap.add_argument("--batched-instances", type=int, default=64, help="instances of the batched leg")
-    ap.add_argument("--served-requests", type=int, default=40, help="requests of the served leg's sample")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched, served and precision legs")
+    ap.add_argument("--batched-instances", type=int, default=64, help="instances of the batched leg (per rank)")
+    ap.add_argument("--served-requests", type=int, default=12, help="requests of the FP32 served leg's sample")
+    ap.add_argument("--served-requests-fp64", type=int, default=6, help="requests of the FP64 served leg's sample")
     args = ap.parse_args()
+    if args.profile_passes:
+        profile_workload(args.profile_passes, args.round_trips, args.plane)
+        return
     args.warmup = max(3, args.warmup) if args.impl == "ours" else args.warmup
     if args.impl == "reference":
         run_reference(args)

@@ -113,6 +113,8 @@ def lib():
         L.opo_get_tuning.argtypes = [vp, ctypes.POINTER(_i)]
         L.opo_set_tuning.argtypes = [vp, ctypes.POINTER(_i)]
         L.opo_field_sums_noalloc.argtypes = [vp, vp, vp, ctypes.c_size_t, _i, vp, dp]
+        L.opo_noalloc_last_error.argtypes = []
+        L.opo_noalloc_last_error.restype = ctypes.c_char_p
         L.opo_set_pass_timing.argtypes = [vp, _i]
         L.opo_pass_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong)]
         L.opo_round_trip_index.argtypes = [vp]
@@ -254,7 +256,8 @@ class Simulation:
         return st.value or 0
 
     def autotune(self):
-        """Pick the fastest kernel variant and tile per pass (zeroes Ap, As, Ai)."""
+        """Pick the fastest kernel variant and tile per pass (timed on scratch fields; the
+        solver's fields are left as they were)."""
         self._check(lib().opo_autotune(self._h))
         return self.tuning
 

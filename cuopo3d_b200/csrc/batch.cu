@@ -569,15 +569,17 @@ int opo_batch_add(OpoBatch *b, const OpoParams *p, const double *w, int *slot_ou
     if (!b || !p || !w || !slot_out) return OPO_ERR_INVALID;
     *slot_out = -1;
     if (p->precision != b->precision) return bfail(b, OPO_ERR_INVALID, "instance precision differs from the batch");
+    // every resident instance takes the same number of z-steps (one round-trip graph);
+    // an instance with another count waits until the batch has drained
     if (!b->order.empty() && p->n_steps != b->n_steps)
-        return bfail(b, OPO_ERR_INVALID, "every instance of a batch takes the same number of z-steps");
+        return bfail(b, OPO_ERR_CAPACITY, "the resident instances take another number of z-steps");
     int free_slot = -1;
     for (int k = 0; k < b->capacity; k++)
         if (!b->slots[k].used) { free_slot = k; break; }
     if (free_slot < 0) return bfail(b, OPO_ERR_CAPACITY, "no free slot");
     const size_t esz = b->precision == OPO_FP64 ? 16 : 8;
     const size_t V = (size_t)p->nx * p->ny * p->nt;
-    const size_t need = 4 * esz * V + (size_t)(1 << 20);  // fields + tables and plans
+    const size_t need = opo::batch_instance_bytes(b->precision, V);  // fields + tables and plans
     if (b->used + need > b->budget) return bfail(b, OPO_ERR_CAPACITY, "HBM budget exhausted");
     OpoSolver *s = nullptr;
     int rc = opo::solver_create_configured(p, w, b->v, b->te, b->stream, &s);

@@ -1182,6 +1182,27 @@ template <typename C> int autotune(OpoSolver *s)
                 return configure_plane<C>(s, e.plane[0], e.plane[1], e.plane[2]);
             }
     }
+    // The candidates are timed on scratch fields (zeroed, so no non-finite values), not on
+    // the caller's: the fields are left as they were, as on a cache hit.  The guard puts
+    // the caller's fields back and frees the scratch on every way out.
+    struct ScratchFields {
+        OpoSolver *s;
+        void *mem = nullptr;
+        void *saved[4] = {};
+        ~ScratchFields()
+        {
+            if (!mem) return;
+            for (int k = 0; k < 4; k++) s->field[k] = saved[k];
+            cudaStreamSynchronize(s->stream);
+            cudaFree(mem);
+        }
+    } scratch{s};
+    OPO_CU(s, cudaMalloc(&scratch.mem, 4 * s->esz * s->V), "cudaMalloc(autotune scratch fields)");
+    OPO_CU(s, cudaMemsetAsync(scratch.mem, 0, 4 * s->esz * s->V, s->stream), "memset(autotune scratch)");
+    for (int k = 0; k < 4; k++) {
+        scratch.saved[k] = s->field[k];
+        s->field[k] = static_cast<char *>(scratch.mem) + k * s->esz * s->V;
+    }
     TuneEntry best{key, {}, {}, {0, 256, 8}};
     const size_t tes[3] = {fp64 ? 512u : 1024u, fp64 ? 1024u : 2048u, fp64 ? 2048u : 4096u};
     const int threads[4] = {128, 256, 160, 288};  // 160 / 288: warp-specialised
@@ -1234,9 +1255,15 @@ template <typename C> int autotune(OpoSolver *s)
         if ((rc = configure_plane<C>(s, best.plane[0], best.plane[1], best.plane[2]))) return rc;
     }
     s->launches = launches0;
-    // the timed passes ran on the resident fields: leave them zeroed
-    for (int k = 1; k < 4; k++) OPO_CU(s, cudaMemsetAsync(s->field[k], 0, s->esz * s->V, s->stream), "memset");
+    // back on the caller's fields: configure the chosen passes again, so that the tensor
+    // maps of the warp-specialised kernels address those fields, not the scratch
     OPO_CU(s, cudaStreamSynchronize(s->stream), "autotune sync");
+    for (int k = 0; k < 4; k++) s->field[k] = scratch.saved[k];
+    for (int k = 0; k < 3; k++) {
+        int rc = configure_pass<C>(s, k, best.v[k], best.te[k]);
+        if (rc) return rc;
+    }
+    if (int rc = configure_plane<C>(s, best.plane[0], best.plane[1], best.plane[2])) return rc;
     std::lock_guard<std::mutex> lock(g_tune_mu);
     g_tune_cache.push_back(best);
     return OPO_OK;

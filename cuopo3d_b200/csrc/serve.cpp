@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/cuopo3d.h"
+#include "solver_internal.h"
 
 namespace {
 
@@ -84,8 +85,7 @@ extern "C" int opo_serve(const OpoServeRequest *reqs, int n, const OpoServeOptio
                 finish(r, OPO_ERR_INVALID, 0, nullptr);
                 continue;
             }
-            const size_t esz = opt->precision == OPO_FP64 ? 16 : 8;
-            if (4 * esz * (size_t)p.nx * p.ny * p.nt > opt->hbm_budget) {
+            if (opo::batch_instance_bytes(opt->precision, (size_t)p.nx * p.ny * p.nt) > opt->hbm_budget) {
                 waiting.pop_front();
                 finish(r, OPO_ERR_CAPACITY, 0, nullptr);
                 continue;
@@ -94,7 +94,15 @@ extern "C" int opo_serve(const OpoServeRequest *reqs, int n, const OpoServeOptio
             opo_time_freq(p.nt, p.t_window, nullptr, w.data());
             int slot = -1;
             rc = opo_batch_add(b, &p, w.data(), &slot);
-            if (rc == OPO_ERR_CAPACITY) break;  // wait for a retirement
+            if (rc == OPO_ERR_CAPACITY) {
+                // no slot, no memory, or another z-step count than the resident instances:
+                // wait for a retirement -- unless nothing is resident, when no retirement
+                // can ever make room
+                if (!live.empty()) break;
+                waiting.pop_front();
+                finish(r, OPO_ERR_CAPACITY, 0, nullptr);
+                continue;
+            }
             if (rc == OPO_ERR_INVALID) {
                 waiting.pop_front();
                 finish(r, OPO_ERR_INVALID, 0, nullptr);

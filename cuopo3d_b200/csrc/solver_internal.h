@@ -7,6 +7,15 @@
 
 namespace opo {
 
+// Device bytes a batch charges one instance against its HBM budget: the four fields
+// (Api, Ap, As, Ai) of nx ny nt complex values plus 1 MiB for its plans and tables.
+// The serving loop's admission uses the same count.
+inline size_t batch_instance_bytes(int precision, size_t voxels)
+{
+    const size_t esz = precision == OPO_FP64 ? 16 : 8;
+    return 4 * esz * voxels + ((size_t)1 << 20);
+}
+
 // Create a solver with the given kernel variant and tile size per pass (t, x, y);
 // `stream` (may be null) replaces the solver's own stream, e.g. a batch's stream.
 int solver_create_configured(const OpoParams *p, const double *w, const PassVariant v[3], const size_t te[3],

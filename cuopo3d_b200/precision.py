@@ -64,3 +64,32 @@ def error_vs_round_trip(kw, checkpoints, seed=1, noise_rel=1e-6, tuning32=None, 
         s64.close()
         s32.close()
     return out
+
+
+def error_of_request(cfg_kw, seed, sigma, round_trips, tuning32=None):
+    """Field and output-power error of one served or batched instance: the FP32 precision
+    form against the FP64 plain form, both initialised on the device the way the batch
+    and the serving loop do it (pump, seeded signal noise `sigma`, idler zero) and run
+    for `round_trips`.  A batched or served FP32 result equals the standalone FP32 run
+    bit for bit (tests/test_batch.py, tests/test_serve.py), so this is its error."""
+    recs = {}
+    for prec in (FP64, FP32):
+        cfg = make_config(precision=prec, **cfg_kw)
+        params, _ = derive(cfg)
+        _, w = time_freq(cfg.nt, params.t_window)
+        sim = Simulation(params, w)
+        try:
+            if prec == FP32 and tuning32 is not None:
+                sim.set_tuning(tuning32)
+                sim.set_plane_pass(0)
+            sim.init_fields(cfg, seed, sigma)
+            sim.run_round_trips(round_trips)
+            recs[prec] = ([sim.get_field(k) for k in (FIELD_AP, FIELD_AS, FIELD_AI)], sim.field_sums())
+        finally:
+            sim.close()
+    (f64, p64), (f32, p32) = recs[FP64], recs[FP32]
+    out = {"round_trips": round_trips}
+    for k, name in enumerate(("pump", "signal", "idler")):
+        out[f"{name}_rel_l2"] = rel_l2(f32[k], f64[k])
+    out["signal_power_rel"] = abs(p32[1] / p64[1] - 1) if p64[1] > 0 else float("nan")
+    return out

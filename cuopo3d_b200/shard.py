@@ -53,10 +53,7 @@ def barrier():
         dist.barrier()
 
 
-def sweep(costs, run_one, rank=0, world=1):
-    """Run instance k (run_one(k) -> picklable result) for every k this rank owns and
-    gather {k: result} of all ranks on rank 0 (None elsewhere)."""
-    mine = {k: run_one(k) for k in local_indices(costs, rank, world)}
+def _gather_dict(mine, rank, world):
     dist = _dist()
     if dist is None or world == 1:
         return mine
@@ -68,3 +65,50 @@ def sweep(costs, run_one, rank=0, world=1):
     for part in gathered:
         out.update(part)
     return out
+
+
+def sweep(costs, run_one, rank=0, world=1):
+    """Run instance k (run_one(k) -> picklable result) for every k this rank owns and
+    gather {k: result} of all ranks on rank 0 (None elsewhere)."""
+    mine = {k: run_one(k) for k in local_indices(costs, rank, world)}
+    return _gather_dict(mine, rank, world)
+
+
+def request_cost(req):
+    """Work of a served request: voxels x its round-trip bound (the z-steps of the
+    instances that share a batch are equal)."""
+    c = req["cfg"]
+    return float(c.nx) * c.ny * c.nt * max(1, c.total_rt)
+
+
+def _percentile(v, q):
+    if not v:
+        return 0.0
+    v = sorted(v)
+    pos = q * (len(v) - 1)
+    lo = int(pos)
+    hi = min(lo + 1, len(v) - 1)
+    return v[lo] + (pos - lo) * (v[hi] - v[lo])
+
+
+def serve_sharded(requests, run_share, rank=0, world=1):
+    """The served form on `world` GPUs: requests are assigned to ranks by
+    longest-processing-time first on request_cost, each rank serves its share with
+    run_share(list of requests) -> (results, stats) (cuopo3d_b200.serve on its own GPU,
+    continuous batching within the rank), and rank 0 gets the results in request order
+    and the job's stats: wall = the slowest rank's, voxel-steps summed, p50 / p99 over
+    all requests' latencies.  No data crosses ranks but the results."""
+    costs = [request_cost(r) for r in requests]
+    mine = local_indices(costs, rank, world)
+    res, st = run_share([requests[k] for k in mine]) if mine else ([], {"wall_s": 0.0, "voxel_steps": 0.0})
+    wall = reduce_scalar(st.get("wall_s", 0.0), "max")
+    vsteps = reduce_scalar(st.get("voxel_steps", 0.0), "sum")
+    allres = _gather_dict({k: r for k, r in zip(mine, res)}, rank, world)
+    if allres is None:
+        return None, None
+    ordered = [allres[k] for k in range(len(requests))]
+    lat = [r["latency_s"] for r in ordered if r["status"] == 0]
+    stats = {"p50_latency_s": _percentile(lat, 0.5), "p99_latency_s": _percentile(lat, 0.99), "wall_s": wall,
+             "voxel_steps": vsteps, "voxel_steps_per_s": vsteps / wall if wall > 0 else 0.0,
+             "completed": len(lat), "ranks": world}
+    return ordered, stats

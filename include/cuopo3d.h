@@ -213,8 +213,9 @@ int opo_pass_times(OpoSolver *s, double ms[4], long long counts[4]);
  * time the tuned x + y passes against every fused plane-pass variant (cluster size,
  * CTA size, first-stage radix) and keep the faster diffraction operator; results
  * are cached per (grid, precision, device) for the process, so later solvers of the same
- * shape reuse them without timing.  The timed passes run on the resident pump, signal
- * and idler, which are left zeroed: call it right after opo_create.  Stands in for the
+ * shape reuse them without timing.  The candidates are timed on temporary scratch fields
+ * (4 x nx ny nt complex values, allocated for the call), so the solver's own fields are
+ * left as they were whether or not the cache held the grid.  Stands in for the
  * reference's compile-time block sizes (DtypesConsts.cuh:48-50). */
 int opo_autotune(OpoSolver *s);
 
@@ -256,14 +257,19 @@ int opo_get_stream(const OpoSolver *s, void **stream);
  * call waits for the stream and writes the sums to host memory.  For callers that
  * cannot call cudaMalloc -- hosts whose own allocator has reserved the device memory,
  * or loops that cannot afford an allocation's implicit device synchronisation -- it
- * allocates nothing: its scratch is a fixed 98,328-byte device array inside the library,
+ * allocates nothing: its scratch is a fixed 24,600-byte device array inside the library,
  * held on every device that loads it until exit.  Limit: n <= 268,435,456 values per
- * field, larger n returns OPO_ERR_CAPACITY.  All calls share that array, so calls whose
- * GPU work overlaps race and must be ordered by the caller.  The first call on a device
- * looks up the array's device address; make that first call before any stream capture.
+ * field, larger n returns OPO_ERR_CAPACITY.  Non-finite sums return OPO_ERR_NONFINITE,
+ * like opo_field_sums.  All calls share that array, so calls whose GPU work overlaps race
+ * and must be ordered by the caller.  The first call on a device (and the first after the
+ * device's context was reset) looks up the array's device address; make that first call
+ * before any stream capture.  The result depends only on n (fixed summation order).
  * This entry point has no counterpart in the reference. */
 int opo_field_sums_noalloc(const void *f0, const void *f1, const void *f2, size_t n, int precision,
                            void *stream, double sums[3]);
+/* Message of the calling thread's last failed opo_field_sums_noalloc call ("" after a
+ * successful one).  No counterpart in the reference. */
+const char *opo_noalloc_last_error(void);
 
 /* Measured FP64 arithmetic peak of the current device in TFLOP/s (independent FMA chains
  * on every SM, best of five event-timed launches; allocates a few bytes).  The reference
@@ -290,7 +296,9 @@ const char *opo_version(void);
 typedef struct OpoBatch OpoBatch;
 int opo_batch_create(int precision, int capacity, size_t hbm_budget_bytes, const int tuning[9], OpoBatch **out);
 void opo_batch_destroy(OpoBatch *b);
-/* Admit one instance (OPO_ERR_CAPACITY when no slot or budget is left). */
+/* Admit one instance.  OPO_ERR_CAPACITY when no slot is free, when its fields and tables
+ * (4 x nx ny nt complex values + 1 MiB) do not fit the budget left, or when the resident
+ * instances take another number of z-steps (it fits once the batch has drained). */
 int opo_batch_add(OpoBatch *b, const OpoParams *p, const double *w, int *slot);
 int opo_batch_remove(OpoBatch *b, int slot);
 int opo_batch_set_field(OpoBatch *b, int slot, int which, const void *src, int where, int elem_precision);
@@ -332,7 +340,8 @@ typedef struct OpoServeOptions {
 
 typedef struct OpoServeResult {
     int status;           /* OPO_OK, OPO_ERR_NONFINITE (fields stopped being finite),
-                             OPO_ERR_INVALID (malformed), OPO_ERR_CAPACITY (never fits)   */
+                             OPO_ERR_INVALID (malformed), OPO_ERR_CAPACITY (does not fit
+                             even with nothing else resident)                              */
     int round_trips;
     double admit_s, done_s, latency_s;  /* latency = done - arrival                        */
     double power[3];      /* final FP64 sums of |A|^2 (pump, signal, idler)              */

@@ -1,10 +1,10 @@
 #!/bin/bash
 # Test infrastructure: compiles crystal_scalars.cpp against the reference's crystal
-# headers (reference checkout, default /root/reference) into oracle/_ref/.
+# headers (reference checkout: the argument, else $CUOPO3D_REFERENCE, else /root/reference) into oracle/_ref/.
 # Usage: build_crystal_scalars.sh [reference_root]
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${CUOPO3D_REFERENCE:-/root/reference}}"
 OUT="$HERE/../_ref"
 HDR="$REF/src/headers"
 if [ ! -f "$HDR/CrystalsBase/PPLN.cuh" ]; then

@@ -1,11 +1,11 @@
 #!/bin/bash
 # Test infrastructure: compiles the reference cuOPO3D solver from its own headers
-# (reference checkout, default /root/reference) through ref_harness.cu, once per
+# (reference checkout: the argument, else $CUOPO3D_REFERENCE, else /root/reference) through ref_harness.cu, once per
 # grid / precision / fix set, into oracle/_ref/.  Nothing is copied from the reference;
 # the headers are read where they lie.  Usage: build_ref.sh [reference_root]
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${CUOPO3D_REFERENCE:-/root/reference}}"
 OUT="$HERE/../_ref"
 HDR="$REF/src/headers"
 if [ ! -f "$HDR/Solver3D.cuh" ]; then

@@ -324,8 +324,8 @@ static int run(const Args &a)
             solv->setDiffractionPropagatorsInFreeSpace(cr->Lcr);
             solv->diffractionInFreeSpace();
             if (cav->gdd) { solv->GDDCompensation(A->As); solv->GDDCompensation(A->Ai); }
-            cav->applyReflectivity(A->As, cav->Rs, 0.0f);
-            cav->applyReflectivity(A->Ai, cav->Ri, 0.0f);
+            if (std::get<1>(A->resFields)) cav->applyReflectivity(A->As, cav->Rs, 0.0f);
+            if (std::get<2>(A->resFields)) cav->applyReflectivity(A->Ai, cav->Ri, 0.0f);
             cudaEventRecord(e1);
             CHECK(cudaEventSynchronize(e1));
             float ms = 0;

@@ -7,6 +7,7 @@ import os
 import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+MAX_ORACLE_VOXEL_STEPS = 2e8
 
 
 def fixture_names():
@@ -32,6 +33,13 @@ class Golden:
         self.nz = int(self.scalars["NZ"])
         self.nrt = int(self.scalars["NRT"])
         self.mode = self.args["mode"]
+
+    @property
+    def heavy(self):
+        """Whether replaying this fixture through the CPU oracle takes more than a few
+        seconds (the 128 x 128 x 256, 10-round-trip benchmark case: ~4e9 voxel-steps);
+        such fixtures are compared with the FP64 CUDA path only."""
+        return self.nx * self.ny * self.nt * int(self.scalars["nsteps"]) * max(1, self.nrt) > MAX_ORACLE_VOXEL_STEPS
 
     def initial_fields(self, noise_fn):
         """(s0, i0) regenerated from the recorded seed with the given noise function."""

@@ -10,9 +10,10 @@ import numpy as np
 import pytest
 
 import cuopo3d_b200 as co
+from oracle.refharness.locate import reference_root
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_MAIN = "/root/reference/src/cuOPO3D.cu"
+REF_MAIN = os.path.join(reference_root(), "src", "cuOPO3D.cu")
 DEMO = os.path.join(ROOT, "src", "_build", "cuOPO3D_g16")
 DEMO_FLAGS = ["-DOPO_NX=16", "-DOPO_NT=32", "-DOPO_NZ=12", "-DOPO_NRT=3"]
 

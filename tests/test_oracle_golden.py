@@ -8,18 +8,11 @@ from golden_cases import Golden, fixture_names, rel_l2
 from oracle import pyoracle as po
 
 NAMES = fixture_names()
-# Fixtures whose split-step run takes the oracle more than a few seconds on the host
-# cores (the 128x128x256, 10-round-trip benchmark case: ~4e9 voxel-steps) get their
-# scalars, grids and pump checked here; their output fields are checked against the
-# FP64 CUDA path in tests/test_gpu_parity.py.
-MAX_ORACLE_VOXEL_STEPS = 2e8
-
-
-def heavy(g):
-    return g.nx * g.ny * g.nt * int(g.scalars["nsteps"]) * max(1, g.nrt) > MAX_ORACLE_VOXEL_STEPS
 
 
 def oracle_run(g):
+    """Heavy fixtures (Golden.heavy) get their scalars, grids and pump checked here; their
+    output fields are checked against the FP64 CUDA path in tests/test_gpu_parity.py."""
     flags = po.OR_DISPERSION | po.OR_DIFFRACTION
     if g.asis:
         flags |= po.OR_ASIS_Q1 | po.OR_ASIS_Q2
@@ -27,7 +20,7 @@ def oracle_run(g):
     st = po.Setup(ph)
     s0, i0 = g.initial_fields(po.noise)
     api = st.api_complex()
-    if heavy(g):
+    if g.heavy:
         return st, api, None
     if g.mode == "single":
         out = po.single_pass(st, api, s0, i0)

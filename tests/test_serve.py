@@ -80,3 +80,27 @@ def test_realtime_arrivals_admitted_after_arrival():
         assert r["status"] == co.OPO_OK
         assert r["admit_s"] >= q["arrival_s"] and r["latency_s"] > 0
     assert st["p99_latency_s"] >= st["p50_latency_s"] > 0
+
+
+def test_budget_between_fields_and_fields_plus_tables_is_answered():
+    """A budget above the request's fields but below fields + tables (the 1 MiB a batch
+    charges per instance for plans and tables) cannot ever admit it: the request is
+    answered with OPO_ERR_CAPACITY instead of waiting for a retirement that cannot come."""
+    r = request(2, total_rt=2)
+    fields = 4 * 8 * 32 * 32 * 64
+    res, st = co.serve([r, request(0, total_rt=2)], co.FP32, capacity=2, hbm_budget=fields + (512 << 10),
+                       realtime=False)
+    assert res[0]["status"] == co.OPO_ERR_CAPACITY
+    assert res[1]["status"] == co.OPO_OK  # 16 x 16 x 32: 256 KiB of fields + 1 MiB fit
+    assert st["completed"] == 1
+
+
+def test_requests_with_other_step_counts_wait_for_the_batch_to_drain():
+    """All resident instances share one round-trip graph, so a request with another number
+    of z-steps waits until the resident ones have retired, then runs (not rejected)."""
+    reqs = [request(0, total_rt=2), request(1, total_rt=2, nz=7), request(2, total_rt=2)]
+    res, st = co.serve(reqs, co.FP32, capacity=3, hbm_budget=8 << 30, realtime=False)
+    assert all(x["status"] == co.OPO_OK for x in res)
+    assert res[1]["admit_s"] >= res[0]["done_s"]
+    alone, _ = co.serve([reqs[1]], co.FP32, capacity=1, hbm_budget=8 << 30, realtime=False)
+    assert np.array_equal(alone[0]["power"], res[1]["power"])

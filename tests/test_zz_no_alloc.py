@@ -54,3 +54,28 @@ def test_noalloc_rejects_sizes_beyond_capacity():
     assert rc == co.OPO_ERR_CAPACITY
     rc, out = noalloc_sums([p, p, p], 8, co.FP64)
     assert rc == co.OPO_OK and np.all(out == 0)
+
+
+def test_noalloc_messages_nonfinite_and_many_chunks():
+    """More chunks than blocks (each block strides over several 8,192-value chunks), two
+    calls in a row against the allocating entry point; a NaN gives OPO_ERR_NONFINITE like
+    opo_field_sums; a rejected size leaves a message readable through
+    opo_noalloc_last_error and a good call clears it."""
+    torch = pytest.importorskip("torch")
+    V = 1024 * 8192 + 12345  # 1,026 chunks over 1,024 blocks
+    for call in range(2):
+        fields = [torch.from_numpy(co.noise(7 * call + k + 1, 1.0 + k, V)).to(torch.complex64).cuda()
+                  for k in range(3)]
+        rc, got = noalloc_sums([t.data_ptr() for t in fields], V, co.FP32)
+        assert rc == co.OPO_OK
+        assert co.lib().opo_noalloc_last_error() == b""
+        ref = [float(np.sum(np.abs(t.cpu().numpy().astype(np.complex128)) ** 2)) for t in fields]
+        np.testing.assert_allclose(got, ref, rtol=1e-12, atol=0)
+    fields[1][12345] = float("nan")
+    rc, _ = noalloc_sums([t.data_ptr() for t in fields], V, co.FP32)
+    assert rc == co.OPO_ERR_NONFINITE
+    assert b"non-finite" in co.lib().opo_noalloc_last_error()
+    p = fields[0].data_ptr()
+    rc, _ = noalloc_sums([p, p, p], CAPACITY + 1, co.FP32)
+    assert rc == co.OPO_ERR_CAPACITY
+    assert b"capacity" in co.lib().opo_noalloc_last_error()
