@@ -373,6 +373,8 @@ def run_ours(args):
             line["served"] = served_leg(co, co.FP32, args.served_requests, line["batched"]["value"])
             line["served_fp64"] = served_leg(co, co.FP64, args.served_requests_fp64, line["batched_fp64"]["value"])
             line["precision"] = precision_leg(co)
+        if world == 1 and args.writer:
+            line["writer"] = writer_leg(co)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
@@ -530,6 +532,38 @@ def precision_leg(co, checkpoints=(1, 10, 50, 200)):
             "points": out}
 
 
+def writer_leg(co, nx=128, ny=128, nt=2048):
+    """The output writer (opo_save_fields) on one FP32 field of nx x ny x nt: the reference
+    main's text dumps (nt slice files + nx ny trace files, "_r"/"_i" pairs) and the one-file
+    binary form, into a temporary directory that is removed afterwards."""
+    import shutil
+    import tempfile
+    cfg = co.make_config(**dict(FORM_BASE, nx=nx, ny=ny, nt=nt, P=5.0, w0=60.0, precision=co.FP32))
+    params, _ = co.derive(cfg)
+    _, w = co.time_freq(nt, params.t_window)
+    sim = co.Simulation(params, w)
+    sim.init_fields(cfg, 1, 1e-3)
+    sim.synchronize()
+    out = {"grid": [nx, ny, nt], "precision": "fp32"}
+    d = tempfile.mkdtemp(prefix="opo_writer_")
+    try:
+        t0 = time.perf_counter()
+        sim.save_fields(co.FIELD_AS, os.path.join(d, "As"), binary=True)
+        out["binary_s"] = time.perf_counter() - t0
+        out["binary_bytes"] = os.path.getsize(os.path.join(d, "As.bin"))
+        t0 = time.perf_counter()
+        sim.save_fields(co.FIELD_AS, os.path.join(d, "OutputSignalPower_slice"), os.path.join(d, "As_temporal_x_"))
+        out["text_s"] = time.perf_counter() - t0
+        names = os.listdir(d)
+        out["text_files"] = len(names) - 1
+        out["text_bytes"] = sum(os.path.getsize(os.path.join(d, n)) for n in names) - out["binary_bytes"]
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+        sim.close()
+    out["host_threads"] = min(16, os.cpu_count() or 1)
+    return out
+
+
 def cpu_baseline(z_steps=10):
     """The FP64 CPU oracle (test infrastructure, used here only as the reported CPU
     baseline) on all host cores: z_steps split steps of the same C2 grid."""
@@ -640,6 +674,7 @@ def main():
     ap.add_argument("--batched-instances", type=int, default=64, help="instances of the batched leg (per rank)")
     ap.add_argument("--served-requests", type=int, default=12, help="requests of the FP32 served leg's sample")
     ap.add_argument("--served-requests-fp64", type=int, default=6, help="requests of the FP64 served leg's sample")
+    ap.add_argument("--writer", action="store_true", help="time the output writer on a 128x128x2048 field")
     args = ap.parse_args()
     if args.profile_passes:
         profile_workload(args.profile_passes, args.round_trips, args.plane)

@@ -27,6 +27,7 @@ CRYSTALS = {"ppln": PPLN_ID, "mgospplt": MGOSPPLT_ID, "mgosplt": MGOSPPLT_ID, "m
             "zgp": ZGP_ID}
 FIELD_API, FIELD_AP, FIELD_AS, FIELD_AI = 0, 1, 2, 3
 MEM_HOST, MEM_DEVICE = 0, 1
+FILES_TEXT, FILES_BINARY = 0, 1
 PUMP_MODES = {"waveplane-cw": 0, "waveplane-pulsed": 1, "focused-cw": 2, "focused-pulsed": 3,
               "focused-sech2": 4, "waveplane-sech2": 5}
 SCALAR_NAMES = ("np ns ni vp vs vi b2p b2s b2i b3p b3s b3i dQ dk dx dy dz kp ks ki "
@@ -115,6 +116,13 @@ def lib():
         L.opo_field_sums_noalloc.argtypes = [vp, vp, vp, ctypes.c_size_t, _i, vp, dp]
         L.opo_noalloc_last_error.argtypes = []
         L.opo_noalloc_last_error.restype = ctypes.c_char_p
+        L.opo_run_round_trips_tallied.argtypes = [vp, _i, dp, ctypes.POINTER(_i)]
+        L.opo_power_cut_xy.argtypes = [ctypes.POINTER(OpoConfig), dp, dp]
+        L.opo_sweep.argtypes = [ctypes.POINTER(OpoConfig), vp, _i, vp, dp]
+        L.opo_sweep_threshold.argtypes = [vp, _i, dp, dp, dp]
+        L.opo_sweep_write.argtypes = [ctypes.c_char_p, vp, _i, _i]
+        L.opo_save_fields.argtypes = [vp, _i, ctypes.c_char_p, ctypes.c_char_p, _i]
+        L.opo_set_wait_limit.argtypes = [vp, ctypes.c_longlong]
         L.opo_set_pass_timing.argtypes = [vp, _i]
         L.opo_pass_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong)]
         L.opo_round_trip_index.argtypes = [vp]
@@ -248,6 +256,28 @@ class Simulation:
         self._check(lib().opo_field_sums(self._h, _dptr(s)))
         return s
 
+    def run_round_trips_tallied(self, n):
+        """n round trips with the FP64 tallies (pump, signal, idler sums of |A|^2) after
+        each; stops at the first non-finite round trip.  Returns (tallies [done, 3], rc):
+        rc is OPO_OK or OPO_ERR_NONFINITE (other errors raise)."""
+        t = np.zeros(3 * max(n, 1))
+        done = _i(0)
+        rc = lib().opo_run_round_trips_tallied(self._h, n, _dptr(t), ctypes.byref(done))
+        if rc not in (OPO_OK, OPO_ERR_NONFINITE):
+            self._check(rc)
+        return t[:3 * done.value].reshape(done.value, 3), rc
+
+    def save_fields(self, which, slice_prefix=None, trace_prefix=None, binary=False):
+        """The reference's field dumps from one device-to-host copy (opo_save_fields):
+        text slice / trace files, or one binary file '<slice_prefix>.bin'."""
+        enc = lambda x: None if x is None else str(x).encode()
+        self._check(lib().opo_save_fields(self._h, which, enc(slice_prefix), enc(trace_prefix),
+                                          FILES_BINARY if binary else FILES_TEXT))
+
+    def set_wait_limit(self, cycles):
+        """Bound of the warp-specialised passes' pipeline waits (SM cycles; 0: ~2 s)."""
+        self._check(lib().opo_set_wait_limit(self._h, int(cycles)))
+
     @property
     def stream(self):
         """The solver's cudaStream_t as an integer (e.g. for torch.cuda.ExternalStream)."""
@@ -371,6 +401,85 @@ def serve(requests, precision, capacity, hbm_budget, realtime=True, tuning=None)
     return res, dict(zip(SERVE_STATS, stats))
 
 
+class OpoSweepOptions(ctypes.Structure):
+    _fields_ = [("precision", _i), ("round_trips", _i), ("window", _i), ("seed", ctypes.c_uint64),
+                ("noise_sigma", _d), ("hbm_budget", ctypes.c_size_t), ("capacity", _i), ("tuning_set", _i),
+                ("tuning", _i * 9)]
+
+
+class OpoSweepPoint(ctypes.Structure):
+    _fields_ = [("P", _d), ("w0", _d), ("status", _i), ("round_trips", _i), ("sums", _d * 3),
+                ("power_xy", _d * 3), ("output_power", _d), ("gain", _d), ("above", _i)]
+
+
+def _point_dict(p):
+    return dict(P=p.P, w0=p.w0, status=p.status, round_trips=p.round_trips, sums=np.array(p.sums[:]),
+                power_xy=np.array(p.power_xy[:]), output_power=p.output_power, gain=p.gain, above=bool(p.above))
+
+
+def _points(points):
+    arr = (OpoSweepPoint * max(len(points), 1))()
+    for k, q in enumerate(points):
+        for name, _ in OpoSweepPoint._fields_:
+            v = q[name]
+            if name in ("sums", "power_xy"):
+                getattr(arr[k], name)[:] = list(v)
+            else:
+                setattr(arr[k], name, int(v) if name in ("status", "round_trips", "above") else float(v))
+    return arr
+
+
+def power_cut_xy(cfg, sums):
+    """The reference's averagePowerCutXY of each field from FP64 tallies (opo_power_cut_xy)."""
+    s = np.ascontiguousarray(sums, dtype=np.float64)
+    out = np.zeros(3)
+    rc = lib().opo_power_cut_xy(ctypes.byref(cfg), _dptr(s), _dptr(out))
+    if rc:
+        raise OpoError(rc, "opo_power_cut_xy")
+    return out
+
+
+def sweep(base_cfg, powers, waists, round_trips, window=3, seed=1, noise_sigma=1e-3, hbm_budget=8 << 30,
+          capacity=0, tuning=None):
+    """Threshold sweep (opo_sweep): one OPO per (P, w0) point of base_cfg, each run for
+    round_trips with FP64 tallies after every round trip.  Returns (points, tallies) with
+    tallies[k, r] = the sums after round trip r + 1 of point k."""
+    n = len(powers)
+    assert len(waists) == n
+    pts = (OpoSweepPoint * max(n, 1))()
+    for k in range(n):
+        pts[k].P, pts[k].w0 = float(powers[k]), float(waists[k])
+    opt = OpoSweepOptions()
+    opt.precision, opt.round_trips, opt.window, opt.seed = base_cfg.precision, round_trips, window, seed
+    opt.noise_sigma, opt.hbm_budget, opt.capacity = noise_sigma, int(hbm_budget), capacity
+    if tuning is not None:
+        opt.tuning_set = 1
+        flat = []
+        for k in ("t", "x", "y"):
+            flat += [tuning[k]["threads"], tuning[k]["tile"], tuning[k]["r1"]]
+        opt.tuning = (_i * 9)(*flat)
+    tallies = np.zeros(max(n, 1) * round_trips * 3)
+    rc = lib().opo_sweep(ctypes.byref(base_cfg), pts, n, ctypes.byref(opt), _dptr(tallies))
+    if rc:
+        raise OpoError(rc, "opo_sweep")
+    return [_point_dict(pts[k]) for k in range(n)], tallies[:n * round_trips * 3].reshape(n, round_trips, 3)
+
+
+def sweep_threshold(points):
+    """(P below, P above, estimate) of the threshold among sweep points of one waist, or None."""
+    arr = _points(points)
+    lo, hi, est = _d(), _d(), _d()
+    rc = lib().opo_sweep_threshold(arr, len(points), ctypes.byref(lo), ctypes.byref(hi), ctypes.byref(est))
+    return None if rc else (lo.value, hi.value, est.value)
+
+
+def sweep_write(path, points, append=True):
+    """The reference's saveAppendedValues2Columns format: 'P <tab> output power' per line."""
+    rc = lib().opo_sweep_write(str(path).encode(), _points(points), len(points), 1 if append else 0)
+    if rc:
+        raise OpoError(rc, f"opo_sweep_write({path})")
+
+
 class Batch:
     """Many instances advanced together by one persistent launch per pass
     (opo_batch_* of the C-ABI).  Instances are admitted into slots while they fit the
@@ -465,3 +574,15 @@ class Batch:
 
 
 from .reference_api import Cavity, EFields, MgOsPPLT, PPLN, Solver  # noqa: E402,F401
+
+
+def read_field_file(path):
+    """A field written by opo_save_fields in binary form: (header dict, array [t][y][x])."""
+    with open(path, "rb") as f:
+        raw = f.read()
+    if raw[:8] != b"OPO3DFLD":
+        raise ValueError(f"{path}: not a field file")
+    version, nx, ny, nt, esz, which = np.frombuffer(raw[8:32], dtype=np.int32)
+    dt = np.complex128 if esz == 16 else np.complex64
+    a = np.frombuffer(raw[32:], dtype=dt).reshape(nt, ny, nx)
+    return dict(version=int(version), nx=int(nx), ny=int(ny), nt=int(nt), bytes=int(esz), which=int(which)), a

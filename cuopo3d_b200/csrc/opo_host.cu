@@ -322,6 +322,12 @@ struct OpoSolver {
     PassCfg pass[3];
     PlaneCfg plane;
     int *err_dev = nullptr;  // error word of the warp-specialised passes
+    long long wait_cycles = 0;  // bound of their ring waits (0: the default ~2 s)
+    // Set when a warp-specialised pass gave up a wait: that pass's tiles were not all
+    // written, so the fields are lost.  Cleared once all four fields have been uploaded
+    // again (reloaded: bit per field) or initialised (opo_init_fields).
+    bool fields_lost = false;
+    unsigned reloaded = 0;
     std::vector<double> w;
     double *partials = nullptr, *sums_dev = nullptr;
     int sum_blocks = 0;
@@ -369,8 +375,19 @@ int check_pass_error(OpoSolver *s)
     OPO_CU(s, cudaMemcpy(&code, s->err_dev, sizeof(int), cudaMemcpyDeviceToHost), "error word");
     if (!code) return OPO_OK;
     cudaMemset(s->err_dev, 0, sizeof(int));
+    s->fields_lost = true;
+    s->reloaded = 0;
     return fail(s, OPO_ERR_CUDA, "a warp-specialised pass stopped after a pipeline wait timed out (code " +
-                                     std::to_string(code) + ")");
+                                     std::to_string(code) + "); the fields are lost until all four are uploaded "
+                                     "again or initialised");
+}
+
+// Calls that read or advance the fields fail while they are lost (see fields_lost).
+int require_fields(OpoSolver *s)
+{
+    if (!s->fields_lost) return OPO_OK;
+    return fail(s, OPO_ERR_CUDA, "the fields were lost when a warp-specialised pass gave up a pipeline wait; "
+                                 "upload all four (opo_set_field) or initialise them (opo_init_fields)");
 }
 
 cudaEvent_t take_event(OpoSolver *s)
@@ -605,6 +622,7 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
         opo::WsArgs &w = pc.wsa;
         const size_t es = sizeof(C);
         w = opo::WsArgs{};
+        w.wait_cycles = s->wait_cycles;
         w.nstages = 2;
         w.stage_bytes = (unsigned)pc.smem;
         w.inner_mult = (unsigned)(es / 8);
@@ -1373,6 +1391,20 @@ int opo_params_from_config(const OpoConfig *c, OpoParams *o, double *sc)
     return OPO_OK;
 }
 
+int opo_power_cut_xy(const OpoConfig *cfg, const double sums[3], double power[3])
+{
+    if (!cfg || !sums || !power) return OPO_ERR_INVALID;
+    OpoParams p;
+    double sc[OPO_N_SCALARS];
+    int rc = opo_params_from_config(cfg, &p, sc);
+    if (rc) return rc;
+    // Solver3D.cuh:534: 0.5 EPS0 C ns dx dy / (LX LY) sum |A|^2 (the signal index ns for
+    // every field, as the reference)
+    const double k = 0.5 * kEps0 * kC * sc[1] * p.dx * p.dy / (cfg->LX * cfg->LY);
+    for (int f = 0; f < 3; f++) power[f] = k * sums[f];
+    return OPO_OK;
+}
+
 int opo_time_freq(int nt, double T, double *t, double *w)
 {
     if (nt < 2 || !(T > 0)) return OPO_ERR_INVALID;
@@ -1579,6 +1611,8 @@ int opo_set_field(OpoSolver *s, int which, const void *src, int where, int prec)
         (prec != OPO_FP32 && prec != OPO_FP64))
         return fail(s, OPO_ERR_INVALID, "opo_set_field: bad argument");
     const cudaMemcpyKind kind = where == OPO_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    s->reloaded |= 1u << which;
+    if (s->reloaded == 0xfu) s->fields_lost = false;
     if (prec == s->p.precision) {
         OPO_CU(s, cudaMemcpyAsync(s->field[which], src, s->esz * s->V, kind, s->stream), "set_field copy");
         return OPO_OK;
@@ -1601,6 +1635,7 @@ int opo_get_field(OpoSolver *s, int which, void *dst, int where, int prec)
     if (which < 0 || which > 3 || !dst || (where != OPO_MEM_HOST && where != OPO_MEM_DEVICE) ||
         (prec != OPO_FP32 && prec != OPO_FP64))
         return fail(s, OPO_ERR_INVALID, "opo_get_field: bad argument");
+    if (int rc = require_fields(s)) return rc;
     const cudaMemcpyKind kind = where == OPO_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     if (prec == s->p.precision) {
         OPO_CU(s, cudaMemcpyAsync(dst, s->field[which], s->esz * s->V, kind, s->stream), "get_field copy");
@@ -1625,18 +1660,51 @@ int opo_get_field(OpoSolver *s, int which, void *dst, int where, int prec)
 int opo_run_single_pass(OpoSolver *s)
 {
     if (!s) return OPO_ERR_INVALID;
+    if (int rc = require_fields(s)) return rc;
     return s->p.precision == OPO_FP64 ? enqueue_single_pass<double2>(s) : enqueue_single_pass<float2>(s);
 }
 
 int opo_run_round_trips(OpoSolver *s, int n)
 {
     if (!s || n < 0) return s ? fail(s, OPO_ERR_INVALID, "negative round-trip count") : OPO_ERR_INVALID;
+    if (int rc = require_fields(s)) return rc;
     return s->p.precision == OPO_FP64 ? run_round_trips<double2>(s, n) : run_round_trips<float2>(s, n);
+}
+
+int opo_run_round_trips_tallied(OpoSolver *s, int n, double *tallies, int *done)
+{
+    if (done) *done = 0;
+    if (!s || n < 0) return s ? fail(s, OPO_ERR_INVALID, "negative round-trip count") : OPO_ERR_INVALID;
+    if (int rc = require_fields(s)) return rc;
+    for (int k = 0; k < n; k++) {
+        int rc = s->p.precision == OPO_FP64 ? run_round_trips<double2>(s, 1) : run_round_trips<float2>(s, 1);
+        if (rc) return rc;
+        double sums[3];
+        rc = s->p.precision == OPO_FP64 ? field_sums<double2>(s, sums) : field_sums<float2>(s, sums);
+        if (done) *done = k + 1;
+        if (tallies)
+            for (int f = 0; f < 3; f++) tallies[3 * (size_t)k + f] = sums[f];
+        if (rc == OPO_ERR_NONFINITE)
+            return fail(s, OPO_ERR_NONFINITE, "Simulation failed: non-finite fields after round trip " +
+                                                  std::to_string(s->rt_index));
+        if (rc) return rc;
+    }
+    return OPO_OK;
+}
+
+int opo_set_wait_limit(OpoSolver *s, long long cycles)
+{
+    if (!s || cycles < 0) return s ? fail(s, OPO_ERR_INVALID, "negative wait limit") : OPO_ERR_INVALID;
+    s->wait_cycles = cycles;
+    for (auto &pc : s->pass) pc.wsa.wait_cycles = cycles;
+    drop_graphs(s);  // captured launches hold the old bound
+    return OPO_OK;
 }
 
 int opo_field_sums(OpoSolver *s, double sums[3])
 {
     if (!s || !sums) return s ? fail(s, OPO_ERR_INVALID, "null output") : OPO_ERR_INVALID;
+    if (int rc = require_fields(s)) return rc;
     return s->p.precision == OPO_FP64 ? field_sums<double2>(s, sums) : field_sums<float2>(s, sums);
 }
 
@@ -1676,7 +1744,11 @@ int opo_init_fields(OpoSolver *s, const OpoConfig *cfg, uint64_t seed, double si
 {
     if (!s || !cfg) return s ? fail(s, OPO_ERR_INVALID, "null configuration") : OPO_ERR_INVALID;
     int rc = opo::init_fields_device(s, cfg, seed, sigma, idler_copy, s->stream);
-    if (!rc) s->launches++;
+    if (!rc) {
+        s->launches++;
+        s->fields_lost = false;
+        s->reloaded = 0xfu;
+    }
     return rc;
 }
 

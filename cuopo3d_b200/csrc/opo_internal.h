@@ -144,6 +144,9 @@ struct WsArgs {
     // twiddles (ntw values) and the phase tables of the transformed fields (plan.n values
     // each) before the first tile; 0: the tables are read from global memory
     unsigned tab_off, ntw;
+    // bound of the consumers' and the producer's ring waits in SM clock cycles (0: ~2 s);
+    // the producer's final drain of its issued copies always keeps the ~2 s bound
+    long long wait_cycles;
 };
 
 // Kernel variant of one pass: CTA size and first-stage radix; the largest radix any

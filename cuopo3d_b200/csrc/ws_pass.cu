@@ -55,16 +55,18 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
         : "memory");
     return ok != 0;
 }
-// Wait for the completion of the phase of parity `parity`; false when the bound expires.
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity)
+// Wait for the completion of the phase of parity `parity`; false when the bound
+// (`cycles` SM clock cycles, or kWaitIters polls) expires.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, long long cycles = kWaitCycles)
 {
     const long long t0 = clock64();
     for (unsigned it = 0; it < kWaitIters; it++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (clock64() - t0 > kWaitCycles) break;
+        if (clock64() - t0 > cycles) break;
     }
     return false;
 }
+__device__ __forceinline__ long long ring_wait_cycles(const WsArgs &w) { return w.wait_cycles > 0 ? w.wait_cycles : kWaitCycles; }
 
 __device__ __forceinline__ void tma_tensor_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
                                               unsigned long long *bar)
@@ -143,7 +145,7 @@ __device__ __forceinline__ void producer_loop(const WsArgs &w, const TileGeom &g
         const unsigned s = k % nst, use = k / nst;
         if (use > 0) {
             int got = 1;
-            if (lane == 0) got = mbar_wait(&empty[s], (use - 1) & 1u) ? 1 : 0;
+            if (lane == 0) got = mbar_wait(&empty[s], (use - 1) & 1u, ring_wait_cycles(w)) ? 1 : 0;
             got = __shfl_sync(0xffffffffu, got, 0);
             if (!got) {
                 if (lane == 0) atomicExch(w.err, 1);
@@ -154,7 +156,10 @@ __device__ __forceinline__ void producer_loop(const WsArgs &w, const TileGeom &g
         __syncwarp();
         issue_tile<C>(w, g, tile, mask, maps, rowsrc, stage_ptr<C>(stages, w, s), &full[s], lane);
     }
-    // drain: every issued copy has landed before the CTA may exit (its stages go away)
+    // drain: every issued copy has landed before the CTA may exit (its stages go away);
+    // this wait keeps the full bound whatever ring_wait_cycles is: the copies are issued
+    // and complete within microseconds.  Should it still expire (code 2), copies may land
+    // after the CTA exited, so the host treats every nonzero code as fields lost.
     if (lane == 0)
         for (unsigned j = k > nst ? k - nst : 0; j < k; j++)
             if (!mbar_wait(&full[j % nst], (j / nst) & 1u)) {
@@ -172,7 +177,7 @@ __device__ __forceinline__ void consumer_loop(const WsArgs &w, unsigned ntiles, 
     unsigned k = 0;
     for (unsigned tile = blockIdx.x; tile < ntiles; tile += gridDim.x, k++) {
         const unsigned s = k % w.nstages, use = k / w.nstages;
-        if (!mbar_wait(&full[s], use & 1u)) {
+        if (!mbar_wait(&full[s], use & 1u, ring_wait_cycles(w))) {
             *abort_flag = 1;
             atomicExch(w.err, 3);
         }

@@ -154,6 +154,10 @@ int opo_crystal_dispersion_pol(int crystal, double T, int extraordinary, double 
  * (EFields3D.cuh:319-328): t = linspace(-T/2, T/2), w = 2 pi fftshift(linspace(
  * -nt/(2T), nt/(2T))).  Either pointer may be NULL. */
 int opo_time_freq(int nt, double window, double *t, double *w);
+/* The reference's average power of a field over an (x, y) cut, Solver::averagePowerCutXY
+ * (Solver3D.cuh:527-536), from FP64 tallies sums[f] = sum |A_f|^2 (opo_field_sums,
+ * opo_batch_sums): power[f] = 0.5 eps0 c ns dx dy / (LX LY) sums[f]. */
+int opo_power_cut_xy(const OpoConfig *cfg, const double sums[3], double power[3]);
 
 /* Initial pump field, EFields::setPumpField (EFields3D.cuh:244-296), into
  * Api (interleaved complex128, nx*ny*nt values). */
@@ -197,6 +201,13 @@ int opo_run_round_trips(OpoSolver *s, int n);
  * the reference's averagePowerCutXY (Solver3D.cuh:529-545) is
  * 0.5 eps0 c ns dx dy / (LX LY) times the signal entry. */
 int opo_field_sums(OpoSolver *s, double sums[3]);
+/* n round trips like opo_run_round_trips, each followed by the FP64 tallies of that
+ * round trip's output fields (tallies[3 k + f] = sum |A_f|^2 after round trip k, f = pump,
+ * signal, idler; tallies may be NULL) and the reference's NaN probe (Solver3D.cuh:999-1005):
+ * at the first round trip whose fields are not finite the loop stops and returns
+ * OPO_ERR_NONFINITE.  *done (may be NULL) = round trips run.  One host synchronisation per
+ * round trip (the reference also synchronises every round trip, for its probe). */
+int opo_run_round_trips_tallied(OpoSolver *s, int n, double *tallies, int *done);
 
 /* Per-pass device timing with CUDA events on the solver's stream.  While enabled,
  * passes are launched one by one (round trips are not replayed as graphs) with an event
@@ -276,7 +287,16 @@ const char *opo_noalloc_last_error(void);
  * has no counterpart: it is the denominator of the t-pass's FP64-pipe roofline. */
 int opo_fp64_peak(double *tflops);
 
+/* Waits for the solver's stream.  OPO_ERR_CUDA when a warp-specialised pass gave up one
+ * of its bounded pipeline waits: its tiles were not all written, so the fields are lost
+ * and every call that reads or advances them fails until all four have been uploaded again
+ * (opo_set_field) or initialised (opo_init_fields). */
 int opo_synchronize(OpoSolver *s);
+/* Bound of the warp-specialised passes' pipeline waits in SM clock cycles (0: the default,
+ * about 2 s).  A short bound makes a pass give up and report OPO_ERR_CUDA instead of
+ * waiting; it exists to exercise that error path.  The final drain of copies already
+ * issued keeps the default bound.  No counterpart in the reference. */
+int opo_set_wait_limit(OpoSolver *s, long long cycles);
 int opo_round_trip_index(const OpoSolver *s);
 /* Number of kernels this solver has launched since creation (graph nodes included). */
 long long opo_kernel_launches(const OpoSolver *s);
@@ -354,6 +374,61 @@ typedef struct OpoServeResult {
  * latency s, wall s, voxel-steps/s, most resident at once, kernel launches, voxel-steps,
  * completed}.  The reference's sweep re-runs its binary per point (cuOPO3D.sh:65-86). */
 int opo_serve(const OpoServeRequest *reqs, int n, const OpoServeOptions *opt, OpoServeResult *out, double stats[8]);
+
+/* ---- output files (see writer.cpp) -------------------------------------------------- */
+
+enum { OPO_FILES_TEXT = 0, OPO_FILES_BINARY = 1 };
+/* Writes field `which` (OPO_FIELD_*) with one device-to-host copy.  OPO_FILES_TEXT: the
+ * reference's text dumps (Files.cuh:73-211 as cuOPO3D.cu:75-85 calls them), 20 significant
+ * digits, "_r.dat" / "_i.dat" pairs: for every t, "<slice_prefix><t>" holds the (x, y) slice
+ * as NY rows of NX tab-terminated values (saveMatrixComplex_TimeSlice); for every pixel,
+ * "<trace_prefix><x>_y_<y>" holds its NT values one per line (SaveElectricField_time3D_GPU;
+ * main passes "As_temporal_x_" as the prefix).  Either prefix may be NULL to skip that set.
+ * OPO_FILES_BINARY: one file "<slice_prefix>.bin": a 32-byte header ("OPO3DFLD", then int32
+ * version 1, nx, ny, nt, bytes per complex value, which) and the field [t][y][x] in the
+ * solver's precision.  Files are written by up to 16 host threads. */
+int opo_save_fields(OpoSolver *s, int which, const char *slice_prefix, const char *trace_prefix, int format);
+
+/* ---- threshold sweeps (see sweep.cpp) ---------------------------------------------- */
+
+/* The reference's scan over pump power and waist (cuOPO3D.sh:58-80 runs the binary once
+ * per point; the threshold pairs are appended by saveAppendedValues2Columns, Files.cuh:
+ * 215-233, called at cuOPO3D.cu:88), run as waves of instances on one OpoBatch. */
+typedef struct OpoSweepOptions {
+    int precision;        /* OPO_FP32 / OPO_FP64                                          */
+    int round_trips;      /* round trips per point                                        */
+    int window;           /* the gain is measured over the last `window` round trips      */
+    uint64_t seed;        /* signal noise seed of point k: seed + k (opo_noise)           */
+    double noise_sigma;   /* signal noise standard deviation per component                */
+    size_t hbm_budget;    /* device bytes the resident points may take                    */
+    int capacity;         /* points resident at once (<= 0: all)                          */
+    int tuning_set;       /* 1: use `tuning` for the batch kernels                        */
+    int tuning[9];
+} OpoSweepOptions;
+
+typedef struct OpoSweepPoint {
+    double P, w0;         /* in: pump power (W) and waist (um) of the point               */
+    int status;           /* out: OPO_OK, OPO_ERR_NONFINITE (stopped at that round trip),
+                             OPO_ERR_INVALID / OPO_ERR_CAPACITY (not run)                 */
+    int round_trips;      /* out: round trips run                                         */
+    double sums[3];       /* out: final FP64 sums |A|^2 of pump, signal, idler            */
+    double power_xy[3];   /* out: the reference's averagePowerCutXY of each (opo_power_cut_xy) */
+    double output_power;  /* out: power_xy[signal] x (1 - Rs), the output-coupled signal  */
+    double gain;          /* out: signal round-trip gain (Ps(n) / Ps(n - window))^(1/window) */
+    int above;            /* out: 1 when gain > 1 (above threshold)                       */
+} OpoSweepPoint;
+
+/* Run every point of base with its (P, w0) for opt->round_trips round trips.  tallies (may
+ * be NULL): n x round_trips x 3 FP64 sums, tallies[(k R + r) 3 + f] after round trip r + 1
+ * of point k (NaN after a point stopped). */
+int opo_sweep(const OpoConfig *base, OpoSweepPoint *pts, int n, const OpoSweepOptions *opt, double *tallies);
+/* Threshold bracket of run points (one waist): the largest P below threshold that is under
+ * the smallest P above it, and the power where ln(gain), linear between them, crosses 0.
+ * OPO_ERR_INVALID when the scan does not cross threshold. */
+int opo_sweep_threshold(const OpoSweepPoint *pts, int n, double *p_below, double *p_above, double *p_est);
+/* Writes "P <tab> output_power" per completed point in the format of the reference's
+ * saveAppendedValues2Columns (default stream formatting; append or truncate). */
+int opo_sweep_write(const char *path, const OpoSweepPoint *pts, int n, int append);
 
 #ifdef __cplusplus
 }

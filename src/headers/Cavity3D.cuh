@@ -36,6 +36,7 @@ public:
     {
         OpoMirror f{make_float2(std::sqrt(R) * std::cos(phase), std::sqrt(R) * std::sin(phase))};
         thrust::transform(A.begin(), A.end(), A.begin(), f);
+        opo_files::invalidate();
     }
     void setGDDCompensation(real_t g)
     {

@@ -63,3 +63,16 @@ inline void printGrid()
     std::cout << "\nSpatio-temporal grid:\n        ---> (NT, NX, NY, NZ) = (" << NT << ", " << NX << ", " << NY
               << ", " << NZ << ")\n        ---> SIZE = NT*NX*NY = " << SIZE << "\n" << std::endl;
 }
+
+namespace opo_files {
+// Generation of the drop-in's device fields, for the savers' host snapshots (Files.cuh):
+// bumped by every drop-in member that writes a field (Solver runs, EFields' pump and noise
+// setters, Cavity::applyReflectivity).  Code that writes a field directly between two saves
+// of it calls opo_files::invalidate() so that the next save copies it again.
+inline unsigned long long &generation()
+{
+    static unsigned long long g = 0;
+    return g;
+}
+inline void invalidate() { generation()++; }
+}  // namespace opo_files

@@ -94,6 +94,7 @@ public:
         for (size_t k = 0; k < SIZE; k++) h[k] = make_cuFloatComplex((float)a[2 * k], (float)a[2 * k + 1]);
         Api = h;
         pump_set = true;
+        opo_files::invalidate();
         std::cout << "        ---> Pump field mode: " << mode << "\n        ---> Pump Power: " << P
                   << " W\n        ---> Beam waist: " << w0 << " um\n" << std::endl;
     }
@@ -110,5 +111,6 @@ public:
         cVech_t h(Vec.size());
         for (size_t k = 0; k < h.size(); k++) h[k] = make_cuFloatComplex((float)a[2 * k], (float)a[2 * k + 1]);
         Vec = h;
+        opo_files::invalidate();
     }
 };

@@ -1,16 +1,59 @@
 // Text writers with the file names and format of cuOPO3D's savers (20 significant
-// digits, "_r.dat" / "_i.dat" pairs).  The device overloads copy only the part a file
-// holds -- one t-slice (contiguous) or one pixel's time trace (strided) -- instead of
-// the whole field for every file.
+// digits, "_r.dat" / "_i.dat" pairs).  The device overloads read a host snapshot of the
+// field, taken with one device-to-host copy and reused by every later save of the same
+// field while no drop-in member has written the fields since (main's loops over NT slices
+// and NX NY pixels then cost one copy per field, not one per file).  Numbers are formatted
+// with std::to_chars to the digits of "%.20g", which is what the reference's
+// setprecision(20) streams print.
 #pragma once
+
+#include <charconv>
 
 #include "Common.cuh"
 
 namespace opo_files {
+struct Snapshot {
+    const void *ptr = nullptr;
+    size_t n = 0;
+    unsigned long long gen = ~0ull;
+    std::vector<complex_t> h;
+};
+// Host copy of device field V (the four most recent fields are kept).
+inline const std::vector<complex_t> &snapshot(const cVecd_t &V)
+{
+    static Snapshot cache[4];
+    static unsigned next = 0;
+    const void *p = thrust::raw_pointer_cast(V.data());
+    for (auto &c : cache)
+        if (c.ptr == p && c.n == V.size() && c.gen == generation()) return c.h;
+    Snapshot &c = cache[next++ % 4];
+    c.ptr = p;
+    c.n = V.size();
+    c.gen = generation();
+    c.h.resize(V.size());
+    CHECK(cudaMemcpy(c.h.data(), p, sizeof(complex_t) * V.size(), cudaMemcpyDeviceToHost));
+    return c.h;
+}
+
+inline void put20(std::string &out, double v)
+{
+    char buf[64];
+    const auto r = std::to_chars(buf, buf + sizeof(buf), v, std::chars_format::general, 20);
+    out.append(buf, r.ptr);
+}
+inline void write_text(const std::string &name, const std::string &s)
+{
+    std::ofstream f(name, std::ios::binary);
+    f << s;
+}
 inline void write_column(const std::string &name, const std::vector<double> &v)
 {
-    std::ofstream f(name);
-    for (double x : v) f << std::setprecision(20) << x << "\n";
+    std::string s;
+    for (double x : v) {
+        put20(s, x);
+        s += '\n';
+    }
+    write_text(name, s);
 }
 inline void write_pair(const std::string &name, const std::vector<complex_t> &v)
 {
@@ -19,30 +62,26 @@ inline void write_pair(const std::string &name, const std::vector<complex_t> &v)
     write_column(name + "_r.dat", re);
     write_column(name + "_i.dat", im);
 }
-inline void write_matrix(const std::string &name, const std::vector<complex_t> &m)
+// (x, y) slice `slice` of field m (NX NY NT values or one NX NY plane with slice 0)
+inline void write_matrix(const std::string &name, const complex_t *m)
 {
     for (int part = 0; part < 2; part++) {
-        std::ofstream f(name + (part ? "_i.dat" : "_r.dat"));
+        std::string s;
         for (uint32_t iy = 0; iy < NY; iy++) {
-            for (uint32_t ix = 0; ix < NX; ix++)
-                f << std::setprecision(20) << (part ? m[iy * NX + ix].y : m[iy * NX + ix].x) << "\t";
-            f << "\n";
+            for (uint32_t ix = 0; ix < NX; ix++) {
+                put20(s, part ? m[iy * NX + ix].y : m[iy * NX + ix].x);
+                s += '\t';
+            }
+            s += '\n';
         }
+        write_text(name + (part ? "_i.dat" : "_r.dat"), s);
     }
 }
-inline std::vector<complex_t> device_slice(const cVecd_t &V, uint32_t slice)
+inline std::vector<complex_t> trace(const complex_t *V, uint32_t x, uint32_t y)
 {
-    std::vector<complex_t> h(NX * NY);
-    CHECK(cudaMemcpy(h.data(), thrust::raw_pointer_cast(V.data()) + (size_t)slice * NX * NY,
-                     sizeof(complex_t) * NX * NY, cudaMemcpyDeviceToHost));
-    return h;
-}
-inline std::vector<complex_t> device_trace(const cVecd_t &V, uint32_t x, uint32_t y)
-{
-    std::vector<complex_t> h(NT);
-    CHECK(cudaMemcpy2D(h.data(), sizeof(complex_t), thrust::raw_pointer_cast(V.data()) + (size_t)y * NX + x,
-                       sizeof(complex_t) * NX * NY, sizeof(complex_t), NT, cudaMemcpyDeviceToHost));
-    return h;
+    std::vector<complex_t> tr(NT);
+    for (uint32_t t = 0; t < NT; t++) tr[t] = V[IDX(x, y, t)];
+    return tr;
 }
 }  // namespace opo_files
 
@@ -59,12 +98,11 @@ inline void SaveVectorComplexGPU(const cVecd_t &V, std::string name) { SaveVecto
 
 inline void saveMatrixComplex_TimeSlice(const cVech_t &V, uint32_t slice, std::string name)
 {
-    opo_files::write_matrix(name, std::vector<complex_t>(V.begin() + (size_t)slice * NX * NY,
-                                                         V.begin() + (size_t)(slice + 1) * NX * NY));
+    opo_files::write_matrix(name, thrust::raw_pointer_cast(V.data()) + (size_t)slice * NX * NY);
 }
 inline void saveMatrixComplex_TimeSlice(const cVecd_t &V, uint32_t slice, std::string name)
 {
-    opo_files::write_matrix(name, opo_files::device_slice(V, slice));
+    opo_files::write_matrix(name, opo_files::snapshot(V).data() + (size_t)slice * NX * NY);
 }
 inline void saveMatrixComplex_TimeSlice_GPU(const cVecd_t &V, uint32_t slice, std::string name)
 {
@@ -81,13 +119,11 @@ inline void SaveElectricField1D_time_GPU(const cVecd_t &V, std::string name) { S
 
 inline void SaveElectricField3D_time(const cVech_t &V, uint32_t x, uint32_t y, std::string name)
 {
-    std::vector<complex_t> tr(NT);
-    for (uint32_t t = 0; t < NT; t++) tr[t] = V[IDX(x, y, t)];
-    opo_files::write_pair(name, tr);
+    opo_files::write_pair(name, opo_files::trace(thrust::raw_pointer_cast(V.data()), x, y));
 }
 inline void SaveElectricField_time3D_GPU(const cVecd_t &V, uint32_t x, uint32_t y, std::string name)
 {
-    opo_files::write_pair(name, opo_files::device_trace(V, x, y));
+    opo_files::write_pair(name, opo_files::trace(opo_files::snapshot(V).data(), x, y));
 }
 
 inline void saveAppendedValues2Columns(std::string name, real_t a, real_t b)

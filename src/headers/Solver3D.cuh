@@ -115,6 +115,7 @@ private:
             check(opo_get_field(s, which[k], thrust::raw_pointer_cast(vec[k]->data()), OPO_MEM_DEVICE, OPO_FP32), s,
                   "download");
         check(opo_synchronize(s), s, "download");
+        opo_files::invalidate();
         TimingCode(seconds() - t0);
         opo_destroy(s);
     }

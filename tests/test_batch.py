@@ -212,3 +212,26 @@ def test_batch_c4_grid_set_vs_oracle(precision, tol):
         ref = po.round_trips(st, api, api, s0, np.zeros_like(s0), 2)
         for name, a, c in zip(("Ap", "As", "Ai"), got, ref):
             assert rel_l2(a, c) < tol, (kw["nx"], kw["nt"], name, rel_l2(a, c))
+
+
+@pytest.mark.parametrize("mode", sorted(co.PUMP_MODES))
+@pytest.mark.parametrize("precision,tol", [(co.FP64, 1e-13), (co.FP32, 1e-6)])
+def test_device_init_every_pump_mode(mode, precision, tol):
+    """Device field initialisation (init_fields.cu) against the host pump (opo_pump_field,
+    EFields3D.cuh:72-137, 244-296, plus the sech^2 modes) for every mode, on a 3-D grid and,
+    for the plane-wave modes, the 1-D solver's grid (nx = ny = 1, EFields1D.cuh:143-170)."""
+    grids = [(24, 16, 48)] + ([(1, 1, 256)] if mode.startswith("waveplane") else [])
+    for nx, ny, nt in grids:
+        flags = co.DISPERSION | (co.DIFFRACTION if nx > 1 else 0)
+        cfg = co.make_config(nx=nx, ny=ny, nt=nt, nz=4, LX=300.0, LY=300.0, Lcr=3000.0, P=120.0, w0=35.0,
+                             FWHM=3.0, t_window=25.0, pump_mode=mode, flags=flags, precision=precision)
+        params, _ = co.derive(cfg)
+        _, w = co.time_freq(cfg.nt, params.t_window)
+        sim = co.Simulation(params, w)
+        sim.init_fields(cfg, 11, 0.01)
+        for which in (co.FIELD_API, co.FIELD_AP):
+            assert rel_l2(sim.get_field(which), co.pump_field(cfg)) < tol, (mode, nx, which)
+        s = sim.get_field(co.FIELD_AS).ravel()
+        ref = co.noise(11, 0.01, s.size)
+        assert rel_l2(s, ref) < (0 if precision == co.FP64 else 1e-7) or np.array_equal(s, ref)
+        sim.close()

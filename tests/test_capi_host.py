@@ -108,3 +108,42 @@ def test_zloop_step_counts():
         _, sc = co.derive(co.make_config(Lcr=Lcr, nz=nz, zloop_f32=f32))
         assert sc["nsteps"] == expect
         assert po.lib().or_zloop_steps(Lcr, Lcr / (nz - 1.0), f32) == expect
+
+
+def test_power_cut_xy_formula():
+    """opo_power_cut_xy: the reference's averagePowerCutXY (Solver3D.cuh:527-536),
+    0.5 eps0 c ns dx dy / (LX LY) sum |A|^2, with its constants (DtypesConsts.cuh:55-57)."""
+    cfg = co.make_config(nx=32, ny=16, nt=64, nz=5, LX=400.0, LY=300.0, P=2.0)
+    _, sc = co.derive(cfg)
+    sums = np.array([3.0, 0.25, 1e-3])
+    c_um_ps = 299792458 * 1e6 / 1e12
+    eps0 = 8.8541878128e-12 * 1e12 / 1e6
+    want = 0.5 * eps0 * c_um_ps * sc["ns"] * sc["dx"] * sc["dy"] / (400.0 * 300.0) * sums
+    np.testing.assert_allclose(co.power_cut_xy(cfg, sums), want, rtol=1e-14)
+
+
+def _pt(P, gain, status=0, out_p=1.0):
+    return dict(P=P, w0=40.0, status=status, round_trips=12, sums=[0, 0, 0], power_xy=[0, 0, 0],
+                output_power=out_p, gain=gain, above=gain > 1)
+
+
+def test_sweep_threshold_bracket_and_estimate():
+    pts = [_pt(30.0, 1.05), _pt(1.0, 0.90), _pt(10.0, 0.95), _pt(100.0, 2.5), _pt(3000.0, float("nan"), status=4)]
+    lo, hi, est = co.sweep_threshold(pts)
+    assert (lo, hi) == (10.0, 30.0)
+    # ln g linear between the bracket: ln 0.95 + (ln 1.05 - ln 0.95) (P - 10) / 20 = 0
+    want = 10.0 + 20.0 * (0 - np.log(0.95)) / (np.log(1.05) - np.log(0.95))
+    assert est == pytest.approx(want, rel=1e-12) and lo < est < hi
+    assert co.sweep_threshold([_pt(1.0, 0.9), _pt(2.0, 0.95)]) is None  # never crosses
+
+
+def test_sweep_write_reference_format(tmp_path):
+    """'value1 <tab> value2' lines in default stream formatting (saveAppendedValues2Columns,
+    Files.cuh:218-233), completed points only, appended."""
+    path = tmp_path / "Average_power_Waist_40.txt"
+    pts = [_pt(10.0, 0.95, out_p=1.25e-7), _pt(30.0, 1.05, out_p=0.125), _pt(50.0, 1.2, status=4)]
+    co.sweep_write(path, pts, append=True)
+    co.sweep_write(path, pts[:1], append=True)
+    assert open(path).read() == "10\t1.25e-07\n30\t0.125\n10\t1.25e-07\n"
+    co.sweep_write(path, pts[1:2], append=False)
+    assert open(path).read() == "30\t0.125\n"

@@ -77,6 +77,13 @@ def test_dropin_binary_runs_and_matches_library(tmp_path):
         sim.set_field(which, arr)
     sim.run_round_trips(3)
     As = sim.get_field(co.FIELD_AS)
-    for t in (0, 13, 31):
-        got = read_slice(str(tmp_path / f"OutputSignalPower_PumpPower500_W_slice{t}"))
-        assert np.linalg.norm(got - As[t]) <= 1e-4 * np.linalg.norm(As[t])
+    # every slice file and every pixel's trace file (written from one host snapshot of As)
+    files = np.zeros_like(As)
+    for t in range(32):
+        files[t] = read_slice(str(tmp_path / f"OutputSignalPower_PumpPower500_W_slice{t}"))
+        assert np.linalg.norm(files[t] - As[t]) <= 1e-4 * np.linalg.norm(As[t])
+    for x in range(16):
+        for y in range(16):
+            base = str(tmp_path / f"As_temporal_x_{x}_y_{y}")
+            tr = np.loadtxt(base + "_r.dat") + 1j * np.loadtxt(base + "_i.dat")
+            assert np.array_equal(tr, files[:, y, x])  # the traces hold the slices' values

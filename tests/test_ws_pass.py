@@ -115,3 +115,45 @@ def test_ws_variant_refused_where_it_does_not_apply():
     with pytest.raises(co.OpoError):
         sim.set_tuning(dict(before, x=dict(threads=160, tile=2048, r1=8)))
     assert sim.tuning["x"]["threads"] in (128, 256)
+
+
+@pytest.mark.parametrize("precision", [co.FP64, co.FP32])
+def test_wait_expiry_reports_error_and_solver_recovers(precision):
+    """The bounded pipeline waits' error path: with a bound of a few clock cycles the
+    consumers give up their first ring wait (the producer's tensor / bulk copies take far
+    longer), leave together, the producer drains the copies it issued, and the host gets
+    OPO_ERR_CUDA at its next synchronisation.  The fields are then lost: reads and runs
+    fail until all four are uploaded again; with the default bound restored the same
+    solver runs the case again and matches the oracle (the context stays usable)."""
+    grid, tun = FP64_CASES[0]
+    kw = base_kw(*grid)
+    cfg = co.make_config(precision=precision, **kw)
+    params, _ = co.derive(cfg)
+    _, w = co.time_freq(cfg.nt, params.t_window)
+    sim = co.Simulation(params, w)
+    sim.set_tuning(tun)
+    sim.set_plane_pass(0)
+    assert all(sim.tuning[k]["threads"] == 160 for k in "txy")
+    sim.init_fields(cfg, 8, 0.02, idler_copy=True)
+    sim.synchronize()
+    sim.set_wait_limit(4)
+    sim.run_single_pass()
+    with pytest.raises(co.OpoError) as e:
+        sim.synchronize()
+    assert e.value.code == co.OPO_ERR_CUDA and "timed out" in str(e.value)
+    for call in (lambda: sim.get_field(co.FIELD_AS), sim.run_single_pass, sim.field_sums):
+        with pytest.raises(co.OpoError) as e:
+            call()
+        assert e.value.code == co.OPO_ERR_CUDA and "lost" in str(e.value)
+    sim.set_wait_limit(0)
+    api = co.pump_field(cfg)
+    s0 = co.noise(8, 0.02, api.size).reshape(api.shape)
+    for which, arr in ((co.FIELD_API, api), (co.FIELD_AP, api), (co.FIELD_AS, s0), (co.FIELD_AI, s0)):
+        sim.set_field(which, arr)
+    sim.run_round_trips(2)
+    got = [sim.get_field(k) for k in (co.FIELD_AP, co.FIELD_AS, co.FIELD_AI)]
+    sim.synchronize()
+    ref = oracle(kw)
+    tol = 1e-10 if precision == co.FP64 else 1e-5
+    for a, b in zip(got, ref):
+        assert rel_l2(a, b) < tol
