@@ -126,6 +126,8 @@ def test_wait_expiry_reports_error_and_solver_recovers(precision):
     fail until all four are uploaded again; with the default bound restored the same
     solver runs the case again and matches the oracle (the context stays usable)."""
     grid, tun = FP64_CASES[0]
+    if precision == co.FP32:  # FP32 rows of 33 complex64 are not 16-byte strided: classic x-pass
+        tun = dict(tun, x=dict(threads=128, tile=1024, r1=8))
     kw = base_kw(*grid)
     cfg = co.make_config(precision=precision, **kw)
     params, _ = co.derive(cfg)
@@ -133,7 +135,7 @@ def test_wait_expiry_reports_error_and_solver_recovers(precision):
     sim = co.Simulation(params, w)
     sim.set_tuning(tun)
     sim.set_plane_pass(0)
-    assert all(sim.tuning[k]["threads"] == 160 for k in "txy")
+    assert all(sim.tuning[k]["threads"] == tun[k]["threads"] for k in "txy")
     sim.init_fields(cfg, 8, 0.02, idler_copy=True)
     sim.synchronize()
     sim.set_wait_limit(4)
