@@ -638,14 +638,17 @@ PINNED_TUNING = {
 }
 
 
-def profile_workload(precision, round_trips, plane=0):
+def profile_workload(precision, round_trips, plane=0, grid=None):
     """The bench workload with a pinned kernel configuration and no timing, for profilers:
     4 field-conversion kernels (fields uploaded from FP64 host arrays), then per round trip
     n t-passes, n x- and y-passes, the closing t-pass and the free-space x'/y' passes
     (3n + 3 launches; with plane = K the x and y passes are one plane pass: 2n + 2)."""
     import cuopo3d_b200 as co
     prec = co.FP64 if precision == "fp64" else co.FP32
-    cfg = co.make_config(precision=prec, **WORKLOAD)
+    kw = dict(WORKLOAD)
+    if grid:  # a smaller grid of the same physics (tile geometry as long as nx >= the tile's pixels)
+        kw.update(nx=grid[0], ny=grid[1], nt=grid[2])
+    cfg = co.make_config(precision=prec, **kw)
     params, _ = co.derive(cfg)
     _, w = co.time_freq(cfg.nt, params.t_window)
     sim = co.Simulation(params, w)
@@ -665,6 +668,8 @@ def main():
                     help="run the workload with the pinned kernel configuration, untimed (for profilers)")
     ap.add_argument("--round-trips", type=int, default=1, help="round trips of --profile-passes")
     ap.add_argument("--plane", type=int, default=0, help="--profile-passes: plane-pass cluster size (0: x and y)")
+    ap.add_argument("--profile-grid", type=int, nargs=3, metavar=("NX", "NY", "NT"),
+                    help="--profile-passes: grid (default: the workload's 128 128 256)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
@@ -677,7 +682,7 @@ def main():
     ap.add_argument("--writer", action="store_true", help="time the output writer on a 128x128x2048 field")
     args = ap.parse_args()
     if args.profile_passes:
-        profile_workload(args.profile_passes, args.round_trips, args.plane)
+        profile_workload(args.profile_passes, args.round_trips, args.plane, args.profile_grid)
         return
     args.warmup = max(3, args.warmup) if args.impl == "ours" else args.warmup
     if args.impl == "reference":

@@ -563,7 +563,9 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     if ((size_t)n > te) te = pc.te = (size_t)n;  // a tile holds at least one whole line
     std::vector<cd> tw;
     int r1 = v.r1;
-    if (fp64 && kind == kT && r1 > 8) r1 = 8;  // 3 fields x r1 complex128 live in registers
+    // 3 fields x r1 complex128 live in registers in the register form of the t-pass; a
+    // radix-16 first stage runs the split form (coupled-wave sweep, then per-field stages)
+    if (fp64 && kind == kT && r1 > 8 && (opo::is_ws(v) || v.threads != 256)) r1 = 8;
     while (r1 >= 4 && !build_plan(n, r1, opo::variant_max_radix(fp64, v), pc.plan, tw)) r1 /= 2;
     if (r1 < 4) return fail(s, OPO_ERR_INVALID, "grid sizes must be 2^a 3^b and >= 8");
     pc.v.r1 = r1;
@@ -898,7 +900,10 @@ TPassArgs<C> make_tpass_args(OpoSolver *s, bool reset_pump, int n_rk4, const dou
         const double zs[3] = {zh[k], zh[k] + 0.5 * h, zh[k] + h};
         for (int j = 0; j < 3; j++) a.ph[k][j] = to_c<C>(std::polar(1.0, p.dk * zs[j]));
     }
-    a.skip_rows = (p.flags & OPO_ASIS_Q2) ? 1 : 0;
+    // the shipped quirk Q2 is the dispersion step's launch grid (Solver3D.cuh:603-629); the
+    // closing pass's GDD compensation and mirrors act on every pixel (the mirror is a
+    // transform over the whole field, Cavity3D.cuh:12-28)
+    a.skip_rows = ((p.flags & OPO_ASIS_Q2) && which_tab == 0) ? 1 : 0;
     a.nx = (unsigned)p.nx;
     a.eom = which_tab == 1 ? static_cast<const C *>(pc.eom) : nullptr;
     return a;

@@ -171,7 +171,9 @@ inline bool variant_compiled(bool fp64, bool tpass, PassVariant v)
     if (v.threads != 128 && v.threads != 256) return false;
     if (v.r1 != 4 && v.r1 != 8 && v.r1 != 16) return false;
     if (!fp64) return true;
-    if (v.threads == 128 || tpass) return v.r1 <= 8;
+    // FP64: 128-thread CTAs take radix <= 8 (registers); a radix-16 first stage of the
+    // t-pass runs its coupled-wave half steps as a separate sweep (256 threads)
+    if (v.threads == 128) return v.r1 <= 8;
     return true;
 }
 

@@ -373,6 +373,98 @@ __device__ __forceinline__ void rk4_half_fast(const TPassArgs<C> &a, C &p, C &s,
     i = add_iku_w(i, a.h6k[2], Ui);
 }
 
+// The same half step for two voxels at once in FP32, their real parts and imaginary parts
+// each held as one packed f32x2 pair (v[0] = {re of voxel 0, re of voxel 1}, v[1] = the
+// imaginary parts): every product and update then serves both voxels with one packed
+// instruction per component, and a complex product costs 5 instead of 8 instructions
+// for the pair.  u = s i, p i*, p s*;  A + c i kappa u  and  A += (h/6) i kappa (u1 + 2 u2 +
+// 2 u3 + u4)  as in rk4_half_fast.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 x2_mul(f32x2 a, f32x2 b)
+{
+    f32x2 d;
+    asm("mul.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 x2_add(f32x2 a, f32x2 b)
+{
+    f32x2 d;
+    asm("add.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 x2_sub(f32x2 a, f32x2 b)
+{
+    f32x2 d;
+    asm("sub.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 x2_fma(f32x2 a, f32x2 b, f32x2 c)
+{
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ f32x2 x2_dup(float s) { return f2pack(float2{s, s}); }
+// a b (conj_b: a conj(b)) for pairs of complex values in split re / im form
+template <bool CONJ_B>
+__device__ __forceinline__ void x2_cmul(const f32x2 *a, const f32x2 *b, f32x2 *d)
+{
+    if (CONJ_B) {
+        d[0] = x2_fma(a[0], b[0], x2_mul(a[1], b[1]));
+        d[1] = x2_sub(x2_mul(a[1], b[0]), x2_mul(a[0], b[1]));
+    } else {
+        d[0] = x2_sub(x2_mul(a[0], b[0]), x2_mul(a[1], b[1]));
+        d[1] = x2_fma(a[0], b[1], x2_mul(a[1], b[0]));
+    }
+}
+// d = a + i c u  (c = {c, c}, nc = {-c, -c})
+__device__ __forceinline__ void x2_add_iku(const f32x2 *a, f32x2 c, f32x2 nc, const f32x2 *u, f32x2 *d)
+{
+    d[0] = x2_fma(u[1], nc, a[0]);
+    d[1] = x2_fma(u[0], c, a[1]);
+}
+
+__device__ __forceinline__ void rk4_half_fast_x2(const TPassArgs<float2> &a, f32x2 (&p)[2], f32x2 (&s)[2],
+                                                 f32x2 (&i)[2])
+{
+    const f32x2 two = x2_dup(2.f);
+    f32x2 up[2], us[2], ui[2], Up[2], Us[2], Ui[2], p2[2], s2[2], i2[2];
+    x2_cmul<false>(s, i, up);
+    x2_cmul<true>(p, i, us);
+    x2_cmul<true>(p, s, ui);
+#pragma unroll
+    for (int c = 0; c < 2; c++) { Up[c] = up[c]; Us[c] = us[c]; Ui[c] = ui[c]; }
+#pragma unroll
+    for (int st = 1; st < 4; st++) {
+        const float *ck = st < 3 ? a.c1k : a.c3k;
+        x2_add_iku(p, x2_dup(ck[0]), x2_dup(-ck[0]), up, p2);
+        x2_add_iku(s, x2_dup(ck[1]), x2_dup(-ck[1]), us, s2);
+        x2_add_iku(i, x2_dup(ck[2]), x2_dup(-ck[2]), ui, i2);
+        x2_cmul<false>(s2, i2, up);
+        x2_cmul<true>(p2, i2, us);
+        x2_cmul<true>(p2, s2, ui);
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            if (st < 3) {
+                Up[c] = x2_fma(up[c], two, Up[c]);
+                Us[c] = x2_fma(us[c], two, Us[c]);
+                Ui[c] = x2_fma(ui[c], two, Ui[c]);
+            } else {
+                Up[c] = x2_add(Up[c], up[c]);
+                Us[c] = x2_add(Us[c], us[c]);
+                Ui[c] = x2_add(Ui[c], ui[c]);
+            }
+        }
+    }
+    f32x2 t[2];
+    x2_add_iku(p, x2_dup(a.h6k[0]), x2_dup(-a.h6k[0]), Up, t);
+    p[0] = t[0]; p[1] = t[1];
+    x2_add_iku(s, x2_dup(a.h6k[1]), x2_dup(-a.h6k[1]), Us, t);
+    s[0] = t[0]; s[1] = t[1];
+    x2_add_iku(i, x2_dup(a.h6k[2]), x2_dup(-a.h6k[2]), Ui, t);
+    i[0] = t[0]; i[1] = t[1];
+}
+
 template <typename C>
 __device__ __forceinline__ void rk4_half(const TPassArgs<C> &a, int h, C &p, C &s, C &i)
 {
@@ -414,9 +506,106 @@ template <typename C> __device__ __forceinline__ unsigned tpass_load_mask(const 
 // n_rk4 half steps to each voxel, then the first forward stage of every transformed
 // field into its shared-memory region (untransformed fields go back to global).
 
+// Split form of the t-pass for a staged tile and a radix-16 first stage (256 = 16 x 16:
+// the first stage, the fused middle and the last stage -- three register passes over the
+// tile instead of five for radix 8 x 8 x 4).  Sixteen samples of three fields and the RK4
+// state would not fit in registers together, so the coupled-wave half steps (and the EOM)
+// run first as their own sweep over the staged tile, one voxel per thread and item, in
+// place; then the first forward stage runs per field from shared memory like any other
+// stage.  The arithmetic of every voxel is that of the register form.
+template <typename C, int R1, int THREADS, int RMAX, int BAR = 0>
+__device__ __forceinline__ void tpass_tile_split(const TPassArgs<C> &a, unsigned tile, C *sm)
+{
+    const AxisPlan &p = a.plan;
+    const TileGeom &g = a.g;
+    const unsigned n = p.n, P = g.nlines, lsj = g.lsj;
+    const unsigned base = tile_base(g, tile);
+    bool xform = a.tmask != 0;
+    if (a.skip_rows && base >= a.nx) xform = false;  // row y = base / nx != 0
+    const unsigned tmask = xform ? a.tmask : 0u;
+    const unsigned lmask = tpass_load_mask(a);
+    bool swept = false;
+    if constexpr (sizeof(C) == 8) {
+        // FP32: two neighbouring pixels (l, l + 1) per item, their values as packed pairs
+        // (16-byte shared-memory accesses; one packed instruction per component for both)
+        if (g.pairs && !a.use_phase && (a.n_rk4 > 0 || a.eom || (lmask & ~tmask))) {
+            for (unsigned e = 2 * threadIdx.x; e < n * P; e += 2 * THREADS) {
+                const unsigned j = fdiv(g.nl, e), l = e - j * P;  // time sample j, pixels l, l + 1
+                const unsigned off = l + prow(g, j) * lsj;
+                f32x2 v[3][2];
+#pragma unroll
+                for (int f = 0; f < 3; f++) {
+                    float4 q4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (lmask & (1u << f)) q4 = *reinterpret_cast<const float4 *>(sm + (size_t)f * g.region + off);
+                    v[f][0] = f2pack(float2{q4.x, q4.z});
+                    v[f][1] = f2pack(float2{q4.y, q4.w});
+                }
+                for (int h = 0; h < a.n_rk4; h++)
+                    rk4_half_fast_x2(reinterpret_cast<const TPassArgs<float2> &>(a), v[0], v[1], v[2]);
+                if (a.eom) {
+                    const C ev = __ldg(a.eom + j);
+                    const f32x2 er = x2_dup(ev.x), ei = x2_dup(ev.y);
+                    for (int f = 1; f < 3; f++) {
+                        const f32x2 re = x2_sub(x2_mul(v[f][0], er), x2_mul(v[f][1], ei));
+                        v[f][1] = x2_fma(v[f][0], ei, x2_mul(v[f][1], er));
+                        v[f][0] = re;
+                    }
+                }
+                const unsigned gb = base + l * g.gs_l + j * g.gs_j;
+#pragma unroll
+                for (int f = 0; f < 3; f++) {
+                    const float2 re = f2unpack(v[f][0]), im = f2unpack(v[f][1]);
+                    const float4 q4 = make_float4(re.x, im.x, re.y, im.y);
+                    if (tmask & (1u << f))
+                        *reinterpret_cast<float4 *>(sm + (size_t)f * g.region + off) = q4;
+                    else if (lmask & (1u << f))
+                        *reinterpret_cast<float4 *>(a.f[f] + gb) = q4;
+                }
+            }
+            tile_sync<BAR>();
+            swept = true;
+        }
+    }
+    if (!swept && (a.n_rk4 > 0 || a.eom || (lmask & ~tmask))) {
+        for (unsigned e = threadIdx.x; e < n * P; e += THREADS) {
+            const unsigned j = fdiv(g.nl, e), l = e - j * P;  // time sample j of pixel l
+            const unsigned off = l + prow(g, j) * lsj;
+            C v[3];
+#pragma unroll
+            for (int f = 0; f < 3; f++) v[f] = (lmask & (1u << f)) ? sm[(size_t)f * g.region + off] : C{};
+            for (int h = 0; h < a.n_rk4; h++) rk4_half(a, h, v[0], v[1], v[2]);
+            if (a.eom) {
+                const C ev = __ldg(a.eom + j);
+                v[1] = cmul(v[1], ev);
+                v[2] = cmul(v[2], ev);
+            }
+            const unsigned gb = base + l * g.gs_l + j * g.gs_j;
+#pragma unroll
+            for (int f = 0; f < 3; f++) {
+                if (tmask & (1u << f))
+                    sm[(size_t)f * g.region + off] = v[f];
+                else if (lmask & (1u << f))
+                    a.f[f][gb] = v[f];
+            }
+        }
+        tile_sync<BAR>();
+    }
+    if (!tmask) return;
+    smem_stage_dispatch<C, +1, false, THREADS, RMAX, (BAR > 0)>(p.radix[0], sm, g, (int)n, p.len[0], p.q[0], a.tw,
+                                                               tmask);
+    tile_sync<BAR>();
+    middle_stages<C, +1, THREADS, RMAX, BAR>(sm, g, p, a.tw, a.tab, tmask);
+    final_stage<C, R1, -1, false, THREADS, (BAR > 0)>(sm, g, n, base, a.f, a.tw, p.q[0], tmask);
+    tile_sync<BAR>();
+}
+
 template <typename C, int R1, int THREADS, int RMAX, bool STAGED = false, int BAR = 0>
 __device__ __forceinline__ void tpass_tile(const TPassArgs<C> &a, unsigned tile, C *sm)
 {
+    if constexpr (STAGED && R1 >= 16) {
+        tpass_tile_split<C, R1, THREADS, RMAX, BAR>(a, tile, sm);
+        return;
+    }
     const AxisPlan &p = a.plan;
     const TileGeom &g = a.g;
     const unsigned n = p.n, q = n / R1, P = g.nlines, lsj = g.lsj, qs = qrow(g, q) * lsj;

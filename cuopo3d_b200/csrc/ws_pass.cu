@@ -55,11 +55,31 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
         : "memory");
     return ok != 0;
 }
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
 // Wait for the completion of the phase of parity `parity`; false when the bound
-// (`cycles` SM clock cycles, or kWaitIters polls) expires.
+// (`cycles` SM clock cycles, or kWaitIters polls) expires.  try_wait may suspend the
+// thread until the phase completes within a hardware time window, so a bound shorter
+// than the default polls with the non-blocking test_wait instead: then the bound, not
+// that window, ends the wait.
 __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, long long cycles = kWaitCycles)
 {
     const long long t0 = clock64();
+    if (cycles < kWaitCycles) {
+        for (unsigned it = 0; it < kWaitIters; it++) {
+            if (mbar_test_wait(bar, parity)) return true;
+            if (clock64() - t0 > cycles) break;
+        }
+        return false;
+    }
     for (unsigned it = 0; it < kWaitIters; it++) {
         if (mbar_try_wait(bar, parity)) return true;
         if (clock64() - t0 > cycles) break;

@@ -73,6 +73,8 @@ C2_TUNINGS = {
     "classic": {"t": dict(threads=256, tile=2048, r1=8), "x": dict(threads=256, tile=2048, r1=16),
                 "y": dict(threads=128, tile=1024, r1=8)},
     "plane_k4": "plane",
+    "split16": {"t": dict(threads=256, tile=2048, r1=16), "x": dict(threads=160, tile=1024, r1=8),
+                "y": dict(threads=288, tile=2048, r1=8)},
     "autotuned": "autotune",
 }
 
@@ -397,3 +399,39 @@ def test_autotune_leaves_fields_and_results_unchanged():
         ref = run_oracle(kw, co.DISPERSION | co.DIFFRACTION, s0, i0, "opo", 2)
         assert_close(out, ref, FP64_TOL)
         sim.close()
+
+
+SPLIT_CASES = [((32, 32, 256), {}), ((16, 8, 96), {}), ((24, 16, 192), dict(eom_beta=0.4, eom_fpm=0.05)),
+               ((16, 16, 64), dict(flags=co.DISPERSION | co.DIFFRACTION | co.ASIS_Q2)),
+               ((32, 16, 512), dict(flags=co.DISPERSION | co.DIFFRACTION | co.PHYSICS, Lambda=6.5))]
+
+
+@pytest.mark.parametrize("precision", [co.FP64, co.FP32])
+@pytest.mark.parametrize("grid,over", SPLIT_CASES)
+def test_split_tpass_radix16_vs_oracle(precision, grid, over):
+    """The t-pass with a radix-16 first stage runs its coupled-wave half steps as their own
+    sweep over the staged tile and then the first stage per field (the split form): two
+    round trips against the oracle (GDD, mirrors, EOM, the shipped row-0 quirk, corrected
+    physics, radix-3 grids)."""
+    nx, ny, nt = grid
+    kw = dict(nx=nx, ny=ny, nt=nt, nz=4, LX=300.0, LY=250.0, Lcr=3000.0, P=400.0, w0=40.0, FWHM=3.0, t_window=25.0,
+              pump_mode="focused-pulsed", gdd_gamma=0.6, Rs=0.9, total_rt=3, **over)
+    flags = kw.pop("flags", co.DISPERSION | co.DIFFRACTION)
+    cfg = co.make_config(precision=precision, flags=flags, **kw)
+    params, _ = co.derive(cfg)
+    _, w = co.time_freq(nt, params.t_window)
+    sim = co.Simulation(params, w)
+    threads = 256 if precision == co.FP64 else 128
+    tun = {"t": dict(threads=threads, tile=max(nt, 1024), r1=16), "x": dict(threads=128, tile=1024, r1=8),
+           "y": dict(threads=128, tile=1024, r1=8)}
+    sim.set_tuning(tun)
+    sim.set_plane_pass(0)
+    assert sim.tuning["t"]["r1"] == 16
+    s0 = co.noise(31, 0.02, nx * ny * nt).reshape(nt, ny, nx)
+    api = co.pump_field(cfg)
+    for which, arr in ((co.FIELD_API, api), (co.FIELD_AP, api), (co.FIELD_AS, s0), (co.FIELD_AI, s0)):
+        sim.set_field(which, arr)
+    sim.run_round_trips(2)
+    out = (sim.get_field(co.FIELD_AP), sim.get_field(co.FIELD_AS), sim.get_field(co.FIELD_AI))
+    ref = run_oracle(kw, flags, s0, s0, "opo", 2)
+    assert_close(out, ref, FP64_TOL if precision == co.FP64 else FP32_TOL)
