@@ -154,7 +154,7 @@ __global__ void batch_tally_final_kernel(const double *partials, int nslots, dou
 #define OPO_BT_VARIANTS(X)                                                                         \
     X(float2, 128, 4, 16) X(float2, 128, 8, 16) X(float2, 128, 16, 16) X(float2, 256, 4, 16)        \
     X(float2, 256, 8, 16) X(float2, 256, 16, 16) X(double2, 128, 4, 8) X(double2, 128, 8, 8)        \
-    X(double2, 256, 4, 16) X(double2, 256, 8, 16) X(double2, 256, 16, 16)
+    X(double2, 256, 4, 16) X(double2, 256, 8, 16)
 
 #define OPO_BA_VARIANTS(X)                                                                         \
     X(float2, 128, 4, 16) X(float2, 128, 8, 16) X(float2, 128, 16, 16) X(float2, 256, 4, 16)        \

@@ -563,9 +563,7 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     if ((size_t)n > te) te = pc.te = (size_t)n;  // a tile holds at least one whole line
     std::vector<cd> tw;
     int r1 = v.r1;
-    // 3 fields x r1 complex128 live in registers in the register form of the t-pass; a
-    // radix-16 first stage runs the split form (coupled-wave sweep, then per-field stages)
-    if (fp64 && kind == kT && r1 > 8 && (opo::is_ws(v) || v.threads != 256)) r1 = 8;
+    if (fp64 && kind == kT && r1 > 8) r1 = 8;  // 3 fields x r1 complex128 live in registers
     while (r1 >= 4 && !build_plan(n, r1, opo::variant_max_radix(fp64, v), pc.plan, tw)) r1 /= 2;
     if (r1 < 4) return fail(s, OPO_ERR_INVALID, "grid sizes must be 2^a 3^b and >= 8");
     pc.v.r1 = r1;

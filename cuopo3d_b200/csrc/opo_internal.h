@@ -171,9 +171,10 @@ inline bool variant_compiled(bool fp64, bool tpass, PassVariant v)
     if (v.threads != 128 && v.threads != 256) return false;
     if (v.r1 != 4 && v.r1 != 8 && v.r1 != 16) return false;
     if (!fp64) return true;
-    // FP64: 128-thread CTAs take radix <= 8 (registers); a radix-16 first stage of the
-    // t-pass runs its coupled-wave half steps as a separate sweep (256 threads)
-    if (v.threads == 128) return v.r1 <= 8;
+    // FP64: 128-thread CTAs take radix <= 8 (registers); the t-pass's first stage holds
+    // 3 fields x r1 complex128 with the RK4 state, r1 <= 8 (its split form for a radix-16
+    // first stage measured slower in FP64: one dependent FP64 chain per thread)
+    if (v.threads == 128 || tpass) return v.r1 <= 8;
     return true;
 }
 

@@ -4,8 +4,10 @@
 // Every z-step of the reference (Solver3D.cuh:946-960: RK4(dz/2), dispersion,
 // diffraction, RK4(dz/2)) is executed as three passes over the resident fields, each
 // reading and writing the three complex fields once:
-//   t-pass    coupled-wave RK4 half steps (all stages in registers) fused with the
-//             t-axis operator: transform, times the dispersion phase, inverse transform
+//   t-pass    coupled-wave RK4 half steps (all stages in registers; a radix-16 first
+//             stage runs them as a sweep over the staged tile first, tpass_tile_split)
+//             fused with the t-axis operator: transform, times the dispersion phase,
+//             inverse transform
 //   x-pass,   the separable diffraction operator exp(-i dz 2 pi^2 (fx^2 + fy^2) / k)
 //   y-pass    = (x factor) (y factor), one axis per pass.
 // A CTA owns a tile of whole lines of one axis for all three fields, staged in shared
@@ -512,7 +514,9 @@ template <typename C> __device__ __forceinline__ unsigned tpass_load_mask(const 
 // state would not fit in registers together, so the coupled-wave half steps (and the EOM)
 // run first as their own sweep over the staged tile, one voxel per thread and item, in
 // place; then the first forward stage runs per field from shared memory like any other
-// stage.  The arithmetic of every voxel is that of the register form.
+// stage.  The FP32 variants take it (two pixels per item on packed pairs); in FP64 the
+// per-thread dependent chain of a one-voxel sweep measured slower than the register
+// form, so FP64 first stages stay at radix <= 8.
 template <typename C, int R1, int THREADS, int RMAX, int BAR = 0>
 __device__ __forceinline__ void tpass_tile_split(const TPassArgs<C> &a, unsigned tile, C *sm)
 {

@@ -97,7 +97,7 @@ __global__ void convert_f2d_kernel(const float2 *src, double2 *dst, size_t n)
 #define OPO_T_VARIANTS(X)                                                                          \
     X(float2, 128, 4, 16) X(float2, 128, 8, 16) X(float2, 128, 16, 16) X(float2, 256, 4, 16)        \
     X(float2, 256, 8, 16) X(float2, 256, 16, 16) X(double2, 128, 4, 8) X(double2, 128, 8, 8)        \
-    X(double2, 256, 4, 16) X(double2, 256, 8, 16) X(double2, 256, 16, 16)
+    X(double2, 256, 4, 16) X(double2, 256, 8, 16)
 
 #define OPO_A_VARIANTS(X)                                                                          \
     X(float2, 128, 4, 16) X(float2, 128, 8, 16) X(float2, 128, 16, 16) X(float2, 256, 4, 16)        \
