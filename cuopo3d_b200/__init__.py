@@ -354,7 +354,7 @@ class Simulation:
 
 class OpoServeRequest(ctypes.Structure):
     _fields_ = [("cfg", OpoConfig), ("arrival_s", _d), ("seed", ctypes.c_uint64), ("noise_sigma", _d),
-                ("tol", _d)]
+                ("tol", _d), ("out_fields", ctypes.c_void_p * 3)]
 
 
 class OpoServeOptions(ctypes.Structure):
@@ -373,15 +373,23 @@ SERVE_STATS = ("p50_latency_s", "p99_latency_s", "wall_s", "voxel_steps_per_s", 
 
 def serve(requests, precision, capacity, hbm_budget, realtime=True, tuning=None):
     """Run a request stream with continuous batching (opo_serve).  requests: list of
-    dicts with cfg (OpoConfig), arrival_s, seed, noise_sigma, tol.  Returns (results, stats)."""
+    dicts with cfg (OpoConfig), arrival_s, seed, noise_sigma, tol and, optionally,
+    return_fields=True for the final (pump, signal, idler) of that request in its result
+    ("fields").  Returns (results, stats)."""
     n = len(requests)
     reqs = (OpoServeRequest * max(n, 1))()
+    bufs = {}
     for k, r in enumerate(requests):
         reqs[k].cfg = r["cfg"]
         reqs[k].arrival_s = r.get("arrival_s", 0.0)
         reqs[k].seed = r.get("seed", 1)
         reqs[k].noise_sigma = r.get("noise_sigma", 1e-6)
         reqs[k].tol = r.get("tol", 0.0)
+        if r.get("return_fields"):
+            c = r["cfg"]
+            bufs[k] = [np.zeros((c.nt, c.ny, c.nx), np.complex128) for _ in range(3)]
+            for f in range(3):
+                reqs[k].out_fields[f] = bufs[k][f].ctypes.data
     opt = OpoServeOptions()
     opt.precision, opt.capacity, opt.hbm_budget, opt.realtime = precision, capacity, int(hbm_budget), int(realtime)
     if tuning is not None:
@@ -398,6 +406,8 @@ def serve(requests, precision, capacity, hbm_budget, realtime=True, tuning=None)
     res = [dict(status=o.status, round_trips=o.round_trips, admit_s=o.admit_s, done_s=o.done_s,
                 latency_s=o.latency_s, power=np.array(o.power[:]), voxel_steps=o.voxel_steps)
            for o in out[:n]]
+    for k, b in bufs.items():
+        res[k]["fields"] = tuple(b)
     return res, dict(zip(SERVE_STATS, stats))
 
 

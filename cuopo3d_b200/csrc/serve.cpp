@@ -138,6 +138,11 @@ extern "C" int opo_serve(const OpoServeRequest *reqs, int n, const OpoServeOptio
             if (!finite || steady || limit) {
                 OpoParams p;
                 opo_params_from_config(&reqs[L.req].cfg, &p, nullptr);
+                for (int f = 0; f < 3; f++)
+                    if (reqs[L.req].out_fields[f] &&
+                        (rc = opo_batch_get_field(b, L.slot, OPO_FIELD_PUMP + f, reqs[L.req].out_fields[f],
+                                                  OPO_MEM_HOST, OPO_FP64)))
+                        goto fail;
                 out[L.req].voxel_steps = info[0] * (long long)p.n_steps * info[2];
                 total_vs += out[L.req].voxel_steps;
                 finish(L.req, finite ? OPO_OK : OPO_ERR_NONFINITE, (int)info[0], ps);

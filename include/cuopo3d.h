@@ -347,6 +347,9 @@ typedef struct OpoServeRequest {
     uint64_t seed;        /* signal noise seed (opo_noise)                                */
     double noise_sigma;   /* signal noise standard deviation per component                */
     double tol;           /* retire when |dPs/Ps| over one round trip <= tol (<= 0: never) */
+    double *out_fields[3];/* optional host buffers (nx ny nt complex128 each, [t][y][x]) that
+                             receive the final pump, signal and idler at retirement; NULL
+                             entries are skipped                                          */
 } OpoServeRequest;
 
 typedef struct OpoServeOptions {

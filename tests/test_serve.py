@@ -104,3 +104,41 @@ def test_requests_with_other_step_counts_wait_for_the_batch_to_drain():
     assert res[1]["admit_s"] >= res[0]["done_s"]
     alone, _ = co.serve([reqs[1]], co.FP32, capacity=1, hbm_budget=8 << 30, realtime=False)
     assert np.array_equal(alone[0]["power"], res[1]["power"])
+
+
+C5_GRIDS = [(64, 64, 128), (96, 96, 192), (128, 128, 256)]
+
+
+def c5_request(k, total_rt):
+    nx, ny, nt = C5_GRIDS[k % len(C5_GRIDS)]
+    cfg = co.make_config(nx=nx, ny=ny, nt=nt, nz=5, LX=800.0, LY=800.0, Lcr=2000.0, FWHM=2.0, t_window=40.0,
+                         pump_mode="focused-pulsed", P=1.0 + 3.0 * k, w0=40.0 + 5.0 * k, detuning=0.2 * k,
+                         total_rt=total_rt, precision=co.FP32)
+    return dict(cfg=cfg, arrival_s=0.0, seed=50 + k, noise_sigma=1e-3, tol=0.0, return_fields=True)
+
+
+def test_served_fields_same_alone_and_in_mix_on_c5_grids():
+    """The served form's grids (64^2 x 128, 96^2 x 192 with its radix-3 transforms,
+    128^2 x 256): every request's final pump, signal and idler fields -- not only its
+    tallies -- are the same bit for bit alone and in a mix where requests of other grids
+    join and retire around it, and equal a standalone solver's."""
+    reqs = [c5_request(k, 2 + k % 3) for k in range(6)]
+    mixed, st = co.serve(reqs, co.FP32, capacity=4, hbm_budget=8 << 30, realtime=False)
+    assert st["completed"] == 6 and st["max_resident"] == 4
+    for k, r in enumerate(reqs):
+        alone, _ = co.serve([r], co.FP32, capacity=1, hbm_budget=8 << 30, realtime=False)
+        assert alone[0]["round_trips"] == mixed[k]["round_trips"] == 2 + k % 3
+        for a, b in zip(alone[0]["fields"], mixed[k]["fields"]):
+            assert np.array_equal(a, b), k
+    # request 1 (96^2 x 192) against a standalone solver with the batch's kernel variants
+    r = reqs[1]
+    params, _ = co.derive(r["cfg"])
+    _, w = co.time_freq(r["cfg"].nt, params.t_window)
+    sim = co.Simulation(params, w)
+    sim.set_tuning({"t": dict(threads=128, tile=2048, r1=4), "x": dict(threads=128, tile=2048, r1=8),
+                    "y": dict(threads=128, tile=2048, r1=8)})
+    sim.set_plane_pass(0)
+    sim.init_fields(r["cfg"], r["seed"], r["noise_sigma"])
+    sim.run_round_trips(mixed[1]["round_trips"])
+    for which, f in zip((co.FIELD_AP, co.FIELD_AS, co.FIELD_AI), mixed[1]["fields"]):
+        assert np.array_equal(sim.get_field(which), f)
