@@ -631,7 +631,8 @@ def run_reference(args):
 # Pinned kernel configurations of the bench workload (the autotuner's choices on a B200),
 # for profiling runs whose launch order must not depend on a timing-based choice.
 PINNED_TUNING = {
-    "fp32": {"t": dict(threads=128, tile=2048, r1=16), "x": dict(threads=128, tile=2048, r1=8),
+    # t: the line-specialised FP32 t-pass (first-stage radix 16 + the line flag 256)
+    "fp32": {"t": dict(threads=128, tile=2048, r1=16 + 256), "x": dict(threads=128, tile=2048, r1=8),
              "y": dict(threads=128, tile=2048, r1=16)},
     "fp64": {"t": dict(threads=128, tile=1024, r1=4), "x": dict(threads=160, tile=1024, r1=8),
              "y": dict(threads=288, tile=2048, r1=8)},

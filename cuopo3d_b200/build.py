@@ -12,9 +12,9 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libcuopo3d.so")
 OBJDIR = os.path.join(HERE, "_build")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in ("ssfm_kernels.cu", "opo_host.cu", "noalloc_sums.cu", "batch.cu",
-                                                             "init_fields.cu", "serve.cpp", "sweep.cpp", "writer.cpp", "plane_pass.cu", "ws_pass.cu",
+                                                             "init_fields.cu", "serve.cpp", "sweep.cpp", "writer.cpp", "plane_pass.cu", "ws_pass.cu", "tpass_line.cu",
                                                                      "peaks.cu")]
-HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fft_radix.cuh", "fft_gain.h", "opo_internal.h", "pass_body.cuh",
+HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fft_radix.cuh", "fft_gain.h", "opo_internal.h", "pass_body.cuh", "tpass_line.cuh",
                                                    "solver_internal.h")] + [
     os.path.join(ROOT, "include", "cuopo3d.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "pass_body.cuh"
+#include "tpass_line.cuh"
 #include "solver_internal.h"
 
 namespace opo {
@@ -75,6 +76,42 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 4 : 1)
         const C *src[3] = {d->psrc, d->f[1], d->f[2]};
         stage_tile<C, THREADS, false>(d->g, (unsigned)d->plan.n, tile, src, tpass_load_mask(*d), sm);
         tpass_tile<C, R1, THREADS, RMAX, true>(*d, tile, sm);
+    }
+}
+
+// Batched line-specialised FP32 t-pass: instances whose grid has a line form (line_nt)
+// run that body, the others the generic body of the same CTA size and first-stage radix.
+template <int R1, int THREADS>
+__global__ void __launch_bounds__(THREADS, 4)
+    tpass_line_batch_kernel(const TPassArgs<float2> *descs, const unsigned *prefix, const BatchHeader *hdr, int tp)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TPassArgs<float2> *d = reinterpret_cast<TPassArgs<float2> *>(smem_raw);
+    float2 *sm = reinterpret_cast<float2 *>(smem_raw + desc_bytes<TPassArgs<float2>>());
+    const unsigned ninst = hdr->ninst, total = hdr->total_tiles;
+    int cur = -1;
+    for (unsigned gt = blockIdx.x; gt < total; gt += gridDim.x) {
+        const int i = find_inst(prefix, ninst, gt);
+        if (i != cur) {
+            __syncthreads();
+            stage_desc(descs + i, d);
+            __syncthreads();
+            if (threadIdx.x < 6 && d->ph_steps) d->ph[threadIdx.x / 3][threadIdx.x % 3] = d->ph_steps[tp * 6 + threadIdx.x];
+            __syncthreads();
+            cur = i;
+        }
+        const unsigned tile = gt - __ldg(prefix + i);
+        if (R1 == 16 && d->line_nt == 256) {
+            if constexpr (R1 == 16) tpass_line_tile<256, 16, THREADS>(*d, tile, sm);
+        } else if (R1 == 16 && d->line_nt == 128) {
+            if constexpr (R1 == 16) tpass_line_tile<128, 16, THREADS>(*d, tile, sm);
+        } else if (R1 == 8 && d->line_nt == 64) {
+            if constexpr (R1 == 8) tpass_line_tile<64, 8, THREADS>(*d, tile, sm);
+        } else {
+            const float2 *src[3] = {d->psrc, d->f[1], d->f[2]};
+            stage_tile<float2, THREADS, false>(d->g, (unsigned)d->plan.n, tile, src, tpass_load_mask(*d), sm);
+            tpass_tile<float2, R1, THREADS, 16, true>(*d, tile, sm);
+        }
     }
 }
 
@@ -164,6 +201,17 @@ __global__ void batch_tally_final_kernel(const double *partials, int nslots, dou
 // Resolves the batched kernel of a variant; returns false if it is not compiled.
 template <typename C> bool batch_t_func(PassVariant v, const void **fn)
 {
+    if (is_line(v)) {
+        if constexpr (!std::is_same<C, float2>::value) return false;
+        if (!line_variant_compiled(v.threads, radix_of(v))) return false;
+        if (v.threads == 128)
+            *fn = radix_of(v) == 16 ? reinterpret_cast<const void *>(tpass_line_batch_kernel<16, 128>)
+                                    : reinterpret_cast<const void *>(tpass_line_batch_kernel<8, 128>);
+        else
+            *fn = radix_of(v) == 16 ? reinterpret_cast<const void *>(tpass_line_batch_kernel<16, 96>)
+                                    : reinterpret_cast<const void *>(tpass_line_batch_kernel<8, 96>);
+        return true;
+    }
     bool ok = false;
 #define OPO_F_T(CC, T, R, RM)                                                                       \
     if constexpr (std::is_same<C, CC>::value) {                                                     \

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <new>
 #include <string>
 #include <vector>
@@ -281,6 +282,7 @@ struct PassCfg {
     opo::TileGeom geo{};
     size_t smem = 0;  // one tile buffer (3 field regions)
     int grid = 0;     // CTAs of the single-instance kernel
+    int line_nt = 0;  // t-pass: the line-specialised kernel's time axis (0: generic kernel)
     void *tw = nullptr;
     void *tab[2][3] = {};
     void *eom = nullptr;  // t-pass: EOM phase per time sample (natural order), or null
@@ -562,14 +564,27 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     const int n = kind == kT ? nt : (kind == kX ? nx : ny);
     if ((size_t)n > te) te = pc.te = (size_t)n;  // a tile holds at least one whole line
     std::vector<cd> tw;
-    int r1 = v.r1;
+    const int form = v.r1 & opo::kLineForm;
+    int r1 = opo::radix_of(v);
     if (fp64 && kind == kT && r1 > 8) r1 = 8;  // 3 fields x r1 complex128 live in registers
     while (r1 >= 4 && !build_plan(n, r1, opo::variant_max_radix(fp64, v), pc.plan, tw)) r1 /= 2;
     if (r1 < 4) return fail(s, OPO_ERR_INVALID, "grid sizes must be 2^a 3^b and >= 8");
-    pc.v.r1 = r1;
+    pc.v.r1 = r1 | form;
+    // line-specialised t-pass: a compiled time axis with its two-stage plan, whole pixel
+    // pairs in tiles of 8 pixels, and every pixel transformed (not the shipped Q2 grid)
+    if (form && kind == kT && opo::line_shape(nt, r1) && pc.plan.ns == 2 && nx % opo::kLineP == 0 &&
+        !(p.flags & OPO_ASIS_Q2))
+        pc.line_nt = nt;
     const unsigned nxy = (unsigned)nx * ny;
     opo::TileGeom &g = pc.geo;
-    if (kind == kT) {
+    if (pc.line_nt) {
+        const int P = opo::kLineP;
+        pc.te = (size_t)nt * P;
+        g.nlines = P; g.ntiles = (nx / P) * ny;
+        g.lsl = 1; g.lsj = P; g.region = (unsigned)(opo::tpass_line_smem(nt, r1) / (3 * sizeof(C)));
+        g.tdiv = make_fastdiv(nx / P); g.tmulA = P; g.tmulB = nx; g.gs_j = nxy; g.gs_l = 1;
+        g.pairs = 1;
+    } else if (kind == kT) {
         const int P = largest_divisor_leq(nx, (int)(te / nt));
         g.nlines = P; g.ntiles = (nx / P) * ny;
         g.lsl = 1; g.lsj = P; g.region = (unsigned)(nt * P);
@@ -591,7 +606,7 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
         g.tdiv = make_fastdiv(1); g.tmulA = 0; g.tmulB = (unsigned)rows * nx; g.gs_j = 1; g.gs_l = nx;
     }
     const bool ws = opo::is_ws(v);
-    if (kind != kX && !ws && g.lsj * sizeof(C) < (fp64 ? 128u : 64u)) {
+    if (kind != kX && !ws && !pc.line_nt && g.lsj * sizeof(C) < (fp64 ? 128u : 64u)) {
         // Line groups narrower than a shared-memory wavefront: the last forward stage's
         // butterflies (R rows apart, R its radix) would all fall on the same banks, so
         // one padding row follows every R rows.  Every earlier stage has a stride that
@@ -904,6 +919,7 @@ TPassArgs<C> make_tpass_args(OpoSolver *s, bool reset_pump, int n_rk4, const dou
     a.skip_rows = ((p.flags & OPO_ASIS_Q2) && which_tab == 0) ? 1 : 0;
     a.nx = (unsigned)p.nx;
     a.eom = which_tab == 1 ? static_cast<const C *>(pc.eom) : nullptr;
+    a.line_nt = pc.line_nt;
     return a;
 }
 
@@ -937,8 +953,13 @@ int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, int wh
         OPO_CU(s, opo::launch_tpass_ws<C>(a, w, maps, opo::PassVariant{pc.v.threads - 32, pc.v.r1}, pc.grid, pc.smem,
                                           s->stream),
                "t-pass launch");
+    } else if (opo::is_line(pc.v)) {
+        if constexpr (std::is_same<C, float2>::value)
+            OPO_CU(s, opo::launch_tpass_line(a, pc.v, pc.line_nt, pc.grid, pc.smem, s->stream), "t-pass launch");
     } else {
-        OPO_CU(s, opo::launch_tpass<C>(a, pc.v, pc.grid, pc.smem, s->stream), "t-pass launch");
+        OPO_CU(s, opo::launch_tpass<C>(a, opo::PassVariant{pc.v.threads, opo::radix_of(pc.v)}, pc.grid, pc.smem,
+                                       s->stream),
+               "t-pass launch");
     }
     s->launches++;
     return OPO_OK;
@@ -1249,6 +1270,21 @@ template <typename C> int autotune(OpoSolver *s)
                         best.te[kind] = te;
                     }
                 }
+        // line-specialised FP32 t-pass variants, where the grid has a compiled form
+        for (int r1 : r1s)
+        for (int th : {96, 128}) {
+            const opo::PassVariant lv{th, r1 | opo::kLineForm};
+            if (kind != kT || !opo::variant_compiled(fp64, true, lv)) continue;
+            if (configure_pass<C>(s, kind, lv, tes[0]) != OPO_OK || !s->pass[kind].line_nt) continue;
+            float ms = 0;
+            int rc = time_pass<C>(s, kind, &ms);
+            if (rc) return rc;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best.v[kind] = s->pass[kind].v;
+                best.te[kind] = tes[0];
+            }
+        }
         int rc = configure_pass<C>(s, kind, best.v[kind], best.te[kind]);
         if (rc) return rc;
     }
@@ -1536,7 +1572,8 @@ static int create_impl(const OpoParams *p, const double *w, const opo::PassVaria
         }
         if ((e = opo::configure_kernels(227 * 1024)) != cudaSuccess ||
             (e = opo::configure_plane_kernels(227 * 1024)) != cudaSuccess ||
-            (e = opo::configure_ws_kernels(227 * 1024)) != cudaSuccess) {
+            (e = opo::configure_ws_kernels(227 * 1024)) != cudaSuccess ||
+            (e = opo::configure_line_kernels(227 * 1024)) != cudaSuccess) {
             rc = cuda_fail(s, e, "configure kernels");
             break;
         }
