@@ -79,15 +79,17 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 4 : 1)
     }
 }
 
-// Batched line-specialised FP32 t-pass: instances whose grid has a line form (line_nt)
-// run that body, the others the generic body of the same CTA size and first-stage radix.
-template <int R1, int THREADS>
+// Batched line-specialised t-pass: instances whose grid has a line form (line_nt) run
+// that body (one tile at a time, one tile buffer), the others (FP32 only) the generic
+// body of the same CTA size and first-stage radix.  An FP64 instance without a line body
+// takes radix 4 and is refused by a batch of this variant, so FP64 needs no fallback.
+template <typename C, int R1, int THREADS>
 __global__ void __launch_bounds__(THREADS, 4)
-    tpass_line_batch_kernel(const TPassArgs<float2> *descs, const unsigned *prefix, const BatchHeader *hdr, int tp)
+    tpass_line_batch_kernel(const TPassArgs<C> *descs, const unsigned *prefix, const BatchHeader *hdr, int tp)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    TPassArgs<float2> *d = reinterpret_cast<TPassArgs<float2> *>(smem_raw);
-    float2 *sm = reinterpret_cast<float2 *>(smem_raw + desc_bytes<TPassArgs<float2>>());
+    TPassArgs<C> *d = reinterpret_cast<TPassArgs<C> *>(smem_raw);
+    unsigned char *buf = smem_raw + desc_bytes<TPassArgs<C>>();
     const unsigned ninst = hdr->ninst, total = hdr->total_tiles;
     int cur = -1;
     for (unsigned gt = blockIdx.x; gt < total; gt += gridDim.x) {
@@ -102,15 +104,16 @@ __global__ void __launch_bounds__(THREADS, 4)
         }
         const unsigned tile = gt - __ldg(prefix + i);
         if (R1 == 16 && d->line_nt == 256) {
-            if constexpr (R1 == 16) tpass_line_tile<256, 16, THREADS>(*d, tile, sm);
+            if constexpr (R1 == 16) tpass_line_tile<C, 256, 16, THREADS>(*d, tile, buf);
         } else if (R1 == 16 && d->line_nt == 128) {
-            if constexpr (R1 == 16) tpass_line_tile<128, 16, THREADS>(*d, tile, sm);
+            if constexpr (R1 == 16) tpass_line_tile<C, 128, 16, THREADS>(*d, tile, buf);
         } else if (R1 == 8 && d->line_nt == 64) {
-            if constexpr (R1 == 8) tpass_line_tile<64, 8, THREADS>(*d, tile, sm);
-        } else {
-            const float2 *src[3] = {d->psrc, d->f[1], d->f[2]};
-            stage_tile<float2, THREADS, false>(d->g, (unsigned)d->plan.n, tile, src, tpass_load_mask(*d), sm);
-            tpass_tile<float2, R1, THREADS, 16, true>(*d, tile, sm);
+            if constexpr (R1 == 8) tpass_line_tile<C, 64, 8, THREADS>(*d, tile, buf);
+        } else if constexpr (sizeof(C) == 8) {
+            C *sm = reinterpret_cast<C *>(buf);
+            const C *src[3] = {d->psrc, d->f[1], d->f[2]};
+            stage_tile<C, THREADS, false>(d->g, (unsigned)d->plan.n, tile, src, tpass_load_mask(*d), sm);
+            tpass_tile<C, R1, THREADS, 16, true>(*d, tile, sm);
         }
     }
 }
@@ -202,14 +205,9 @@ __global__ void batch_tally_final_kernel(const double *partials, int nslots, dou
 template <typename C> bool batch_t_func(PassVariant v, const void **fn)
 {
     if (is_line(v)) {
-        if constexpr (!std::is_same<C, float2>::value) return false;
         if (!line_variant_compiled(v.threads, radix_of(v))) return false;
-        if (v.threads == 128)
-            *fn = radix_of(v) == 16 ? reinterpret_cast<const void *>(tpass_line_batch_kernel<16, 128>)
-                                    : reinterpret_cast<const void *>(tpass_line_batch_kernel<8, 128>);
-        else
-            *fn = radix_of(v) == 16 ? reinterpret_cast<const void *>(tpass_line_batch_kernel<16, 96>)
-                                    : reinterpret_cast<const void *>(tpass_line_batch_kernel<8, 96>);
+        *fn = radix_of(v) == 16 ? reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 16, 128>)
+                                : reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 8, 128>);
         return true;
     }
     bool ok = false;

@@ -566,23 +566,23 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     std::vector<cd> tw;
     const int form = v.r1 & opo::kLineForm;
     int r1 = opo::radix_of(v);
-    if (fp64 && kind == kT && r1 > 8) r1 = 8;  // 3 fields x r1 complex128 live in registers
-    while (r1 >= 4 && !build_plan(n, r1, opo::variant_max_radix(fp64, v), pc.plan, tw)) r1 /= 2;
+    // line-specialised t-pass: a compiled time axis with its two-stage plan, whole tiles of
+    // line_pixels() pixels, and every pixel transformed (not the shipped Q2 launch grid)
+    const int LP = opo::line_pixels(fp64);
+    const bool line = form && kind == kT && opo::line_shape(nt, r1) && nx % LP == 0 && !(p.flags & OPO_ASIS_Q2);
+    // 3 fields x r1 complex128 live in registers (the line form's generic fallback: radix 4)
+    if (fp64 && kind == kT && !line) r1 = std::min(r1, form ? 4 : 8);
+    while (r1 >= 4 && !build_plan(n, r1, line ? 16 : opo::variant_max_radix(fp64, v), pc.plan, tw)) r1 /= 2;
     if (r1 < 4) return fail(s, OPO_ERR_INVALID, "grid sizes must be 2^a 3^b and >= 8");
     pc.v.r1 = r1 | form;
-    // line-specialised t-pass: a compiled time axis with its two-stage plan, whole pixel
-    // pairs in tiles of 8 pixels, and every pixel transformed (not the shipped Q2 grid)
-    if (form && kind == kT && opo::line_shape(nt, r1) && pc.plan.ns == 2 && nx % opo::kLineP == 0 &&
-        !(p.flags & OPO_ASIS_Q2))
-        pc.line_nt = nt;
+    if (line && pc.plan.ns == 2 && r1 == opo::radix_of(v)) pc.line_nt = nt;
     const unsigned nxy = (unsigned)nx * ny;
     opo::TileGeom &g = pc.geo;
     if (pc.line_nt) {
-        const int P = opo::kLineP;
-        pc.te = (size_t)nt * P;
-        g.nlines = P; g.ntiles = (nx / P) * ny;
-        g.lsl = 1; g.lsj = P; g.region = (unsigned)(opo::tpass_line_smem(nt, r1) / (3 * sizeof(C)));
-        g.tdiv = make_fastdiv(nx / P); g.tmulA = P; g.tmulB = nx; g.gs_j = nxy; g.gs_l = 1;
+        pc.te = (size_t)nt * LP;
+        g.nlines = LP; g.ntiles = (nx / LP) * ny;
+        g.lsl = 1; g.lsj = LP; g.region = (unsigned)(nt * LP);  // (the kernels lay out their own tiles)
+        g.tdiv = make_fastdiv(nx / LP); g.tmulA = LP; g.tmulB = nx; g.gs_j = nxy; g.gs_l = 1;
         g.pairs = 1;
     } else if (kind == kT) {
         const int P = largest_divisor_leq(nx, (int)(te / nt));
@@ -631,7 +631,7 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
         const unsigned per128 = (unsigned)(128 / sizeof(C));
         g.region = (g.region + per128 - 1) / per128 * per128;
     }
-    pc.smem = 3 * (size_t)g.region * sizeof(C);
+    pc.smem = pc.line_nt ? opo::tpass_line_smem(fp64, nt, r1) : 3 * (size_t)g.region * sizeof(C);
     if (pc.smem > 227 * 1024) return fail(s, OPO_ERR_INVALID, "tile does not fit in shared memory");
     if (ws) {
         opo::WsArgs &w = pc.wsa;
@@ -954,8 +954,7 @@ int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, int wh
                                           s->stream),
                "t-pass launch");
     } else if (opo::is_line(pc.v)) {
-        if constexpr (std::is_same<C, float2>::value)
-            OPO_CU(s, opo::launch_tpass_line(a, pc.v, pc.line_nt, pc.grid, pc.smem, s->stream), "t-pass launch");
+        OPO_CU(s, opo::launch_tpass_line<C>(a, pc.v, pc.line_nt, pc.grid, pc.smem, s->stream), "t-pass launch");
     } else {
         OPO_CU(s, opo::launch_tpass<C>(a, opo::PassVariant{pc.v.threads, opo::radix_of(pc.v)}, pc.grid, pc.smem,
                                        s->stream),
@@ -1271,9 +1270,8 @@ template <typename C> int autotune(OpoSolver *s)
                     }
                 }
         // line-specialised FP32 t-pass variants, where the grid has a compiled form
-        for (int r1 : r1s)
-        for (int th : {96, 128}) {
-            const opo::PassVariant lv{th, r1 | opo::kLineForm};
+        for (int r1 : r1s) {
+            const opo::PassVariant lv{128, r1 | opo::kLineForm};
             if (kind != kT || !opo::variant_compiled(fp64, true, lv)) continue;
             if (configure_pass<C>(s, kind, lv, tes[0]) != OPO_OK || !s->pass[kind].line_nt) continue;
             float ms = 0;

@@ -158,18 +158,22 @@ struct PassVariant {
 };
 
 // Flag in PassVariant::r1 (and in the r1 entries of the C-ABI tuning arrays): the
-// line-specialised FP32 t-pass (tpass_line.cuh: compile-time time axis 64, 128 or 256,
-// tiles of 8 pixels, split-pair arithmetic) with the given first-stage radix, on CTAs of
-// 128 threads or of 96 (one warp per field in the transform stages).  Grids it does not
-// cover (another time axis, nx not a multiple of 8, the shipped Q2 launch grid) run the
-// generic tile body at the same CTA size and radix instead.
+// line-specialised t-pass (tpass_line.cuh: compile-time time axis 64, 128 or 256, tiles
+// of 8 FP32 or 4 FP64 pixels, FP32 split-pair arithmetic) with the given first-stage
+// radix, on CTAs of 128 threads.  Grids it does not cover (another time axis, nx not a
+// multiple of the tile, the shipped Q2 launch grid) run the generic tile body at the
+// same CTA size and radix (FP64: radix 4) instead.
 constexpr int kLineForm = 256;
-constexpr int kLineP = 8;  // pixels per tile of the line-specialised t-pass
+inline int line_pixels(bool fp64) { return fp64 ? 4 : 8; }  // pixels per tile
 inline bool is_line(PassVariant v) { return (v.r1 & kLineForm) != 0; }
 inline int radix_of(PassVariant v) { return v.r1 & (kLineForm - 1); }
 // Line-specialised t-pass kernels: CTA size and first-stage radix; (time axis, radix)
 // pairs with a compiled body.
-inline bool line_variant_compiled(int threads, int r1) { return (threads == 96 || threads == 128) && (r1 == 8 || r1 == 16); }
+inline bool line_variant_compiled(int threads, int r1) { return threads == 128 && (r1 == 8 || r1 == 16); }
+// Largest radix of the generic fallback body at a line variant's CTA size.
+template <typename C, int THREADS> struct LineFallback {
+    static constexpr int RMAX = (sizeof(C) == 16 && THREADS == 128) ? 8 : 16;
+};
 inline bool line_shape(int nt, int r1) { return (nt == 256 && r1 == 16) || (nt == 128 && r1 == 16) || (nt == 64 && r1 == 8); }
 
 inline bool is_ws(PassVariant v) { return v.threads == 160 || v.threads == 288; }
@@ -183,7 +187,7 @@ bool ws_variant_compiled(bool fp64, bool tpass, PassVariant consumers);
 // in ssfm_kernels.cu) for the t-pass (tpass = true) or the axis passes.
 inline bool variant_compiled(bool fp64, bool tpass, PassVariant v)
 {
-    if (is_line(v)) return !fp64 && tpass && line_variant_compiled(v.threads, radix_of(v));
+    if (is_line(v)) return tpass && line_variant_compiled(v.threads, radix_of(v));
     if (is_ws(v)) return ws_variant_compiled(fp64, tpass, PassVariant{v.threads - 32, v.r1});
     if (v.threads != 128 && v.threads != 256) return false;
     if (v.r1 != 4 && v.r1 != 8 && v.r1 != 16) return false;
@@ -199,12 +203,13 @@ inline bool variant_compiled(bool fp64, bool tpass, PassVariant v)
 // cudaErrorInvalidValue for a variant that is not compiled.
 template <typename C> cudaError_t launch_tpass(const TPassArgs<C> &a, PassVariant v, int grid, size_t smem,
                                                cudaStream_t st);
-// Line-specialised FP32 t-pass (v.r1 carries kLineForm) for a time axis of nt samples;
-// nt = 0: the generic tile body at the variant's CTA size and radix.
-cudaError_t launch_tpass_line(const TPassArgs<float2> &a, PassVariant v, int nt, int grid, size_t smem,
+// Line-specialised t-pass (v.r1 carries kLineForm) for a time axis of nt samples; nt = 0:
+// the generic tile body at the variant's CTA size and radix.
+template <typename C>
+cudaError_t launch_tpass_line(const TPassArgs<C> &a, PassVariant v, int nt, int grid, size_t smem,
                               cudaStream_t st);
-// Shared memory of one tile of the line-specialised t-pass (0: nt / r1 not compiled).
-size_t tpass_line_smem(int nt, int r1);
+// Dynamic shared memory of a line-specialised t-pass CTA (0: nt / r1 not compiled).
+size_t tpass_line_smem(bool fp64, int nt, int r1);
 cudaError_t configure_line_kernels(size_t max_smem);
 template <typename C> cudaError_t launch_axis(const AxisArgs<C> &a, PassVariant v, bool bfast, int grid,
                                               size_t smem, cudaStream_t st);

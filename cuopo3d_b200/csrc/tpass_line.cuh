@@ -1,29 +1,28 @@
-// Line-specialised FP32 t-pass: the tile body of tpass_tile / tpass_tile_split for a
-// time axis whose length and radix plan are compile-time constants (NT = RA x RB with
-// RA, RB in {8, 16}: 64, 128, 256) and a tile of P = 8 pixels of one row.
+// Line-specialised t-pass: the tile body of tpass_tile / tpass_tile_split for a time
+// axis whose length and radix plan are compile-time constants (NT = RA x RB with RA, RB
+// in {8, 16}: 64, 128, 256), in FP32 and FP64.
 //
-// It computes what the split t-pass computes (reference Solver3D.cuh:872-943 RK4 half
-// steps, then Solver3D.cuh:572-639 dispersion: transform, phase, inverse transform),
-// with three changes of form:
-//  * every value is held as a split pair: the same time sample of pixels l and l + 1,
-//    real parts in one packed f32x2 register pair and imaginary parts in another, both in
-//    registers and in shared memory (16 bytes: re_l, re_l+1, im_l, im_l+1).  Every
-//    butterfly, twiddle and phase product then serves two lines with one packed
-//    instruction per component: a complex product costs 4 packed instructions for two
-//    values instead of 4 scalar ones for one, and multiplying by +-i only renames
-//    registers;
-//  * each twiddle and phase factor is loaded once for both lines and duplicated into
-//    both lanes of a pair;
-//  * all index arithmetic is compile-time: the tile, the rows and the butterfly of an
-//    item follow from shifts and masks.
-// The transforms are the generic two-stage plan [RA, RB] (decimation in frequency
-// forward, in time inverse, phase tables in the plan's digit-reversed order), so the
-// twiddles and phase tables are the host's tables of that plan.
+// It computes what the generic t-pass computes (reference Solver3D.cuh:872-943 RK4 half
+// steps, then Solver3D.cuh:572-639 dispersion: transform, phase, inverse transform) on
+// tiles of 16-byte units: four units per time sample, one time sample per shared-memory
+// row.  A unit is one FP64 pixel, or in FP32 a split pair: the same time sample of
+// pixels l and l + 1, real parts in one packed f32x2 register pair and imaginary parts
+// in another, in registers and in shared memory (re_l, re_l+1, im_l, im_l+1).  Every FP32
+// butterfly, twiddle and phase product then serves two lines with one packed instruction
+// per component (a complex product: 4 packed instructions for two values; multiplying by
+// +-i only renames registers), each twiddle and phase factor is loaded once for both
+// lines, and all index arithmetic is compile-time.  A tile is 8 pixels (FP32) or 4
+// (FP64) of one row.  The transforms are the generic two-stage plan [RA, RB] (decimation
+// in frequency forward, in time inverse, phase tables in the plan's digit-reversed
+// order), so the twiddles and phase tables are the host's tables of that plan.
 //
-// Shared memory per field: (NT + NT / RB) rows of P / 2 split pairs; time sample t sits
-// in row t + t / RB (a padding row after every RB rows), so the RB-point stage's eight
+// Shared memory per field: NT + NT / RB rows of four units; time sample t sits in row
+// t + t / RB (a padding row after every RB rows), so the RB-point stage's eight
 // butterflies of a warp fall on alternating halves of the banks, and the other stages
 // read whole 512-byte runs.
+//
+// The single-instance kernel runs one tile per CTA, four CTAs of 128 threads per SM; the
+// batched kernel runs the same body over the tiles of every instance.
 #pragma once
 
 #include "pass_body.cuh"
@@ -166,13 +165,6 @@ template <int S> struct XDft<16, S> {
 
 template <int R, int S> __device__ __forceinline__ void xdft(X2C *x) { XDft<R, S>::run(x); }
 
-__device__ __forceinline__ X2C lds_x2c(const float2 *p)
-{
-    const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(p);
-    return X2C{v.x, v.y};
-}
-__device__ __forceinline__ void sts_x2c(float2 *p, X2C v) { *reinterpret_cast<ulonglong2 *>(p) = make_ulonglong2(v.r, v.i); }
-// Interleaved pixel pair {re_l, im_l, re_l+1, im_l+1} <-> split pair
 __device__ __forceinline__ X2C split_of(float4 q)
 {
     return X2C{f2pack(float2{q.x, q.z}), f2pack(float2{q.y, q.w})};
@@ -183,196 +175,276 @@ __device__ __forceinline__ float4 interleaved_of(X2C v)
     return make_float4(re.x, im.x, re.y, im.y);
 }
 
-template <int NT, int RA> struct LineGeom {
-    static constexpr int RB = NT / RA;
-    static constexpr int Q = RB;  // butterflies per line of the RA-point stage
-    static constexpr int PP = kLineP / 2;  // pixel pairs per row
-    static constexpr int ROWS = NT + NT / RB;
-    static constexpr int REGION = ROWS * kLineP;  // float2 elements per field region
-    __device__ __forceinline__ static constexpr int row(int t) { return t + t / RB; }
-    static constexpr size_t smem_bytes() { return 3 * (size_t)REGION * sizeof(float2); }
+// The 16-byte unit of each precision: its register form, loads and stores of the raw
+// layout (the global one, C values interleaved: staged tiles and the fields), the
+// butterflies, table products and the coupled-wave half steps.
+template <typename C> struct LineUnit;
+
+template <> struct LineUnit<float2> {
+    using U = X2C;
+    static constexpr int PX = 2;  // pixels per unit
+    __device__ __forceinline__ static U lds(const void *p)
+    {
+        const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(p);
+        return X2C{v.x, v.y};
+    }
+    __device__ __forceinline__ static void sts(void *p, U v) { *reinterpret_cast<ulonglong2 *>(p) = make_ulonglong2(v.r, v.i); }
+    __device__ __forceinline__ static U load_raw(const void *p) { return split_of(*reinterpret_cast<const float4 *>(p)); }
+    __device__ __forceinline__ static void store_raw(void *p, U v) { *reinterpret_cast<float4 *>(p) = interleaved_of(v); }
+    template <int R, int S> __device__ __forceinline__ static void dft(U *x) { xdft<R, S>(x); }
+    // x t (CONJ: x conj(t)) for a table entry t
+    template <bool CONJ> __device__ __forceinline__ static U tmul(U x, float2 t) { return xmul_tab<CONJ>(x, t); }
+    __device__ __forceinline__ static U zero() { return X2C{0ull, 0ull}; }
+    // n half steps of every voxel of the units p, s, i
+    __device__ __forceinline__ static void rk4(const TPassArgs<float2> &a, U &p, U &s, U &i)
+    {
+        if (!a.use_phase) {
+            f32x2 v[3][2] = {{p.r, p.i}, {s.r, s.i}, {i.r, i.i}};
+            for (int h = 0; h < a.n_rk4; h++) rk4_half_fast_x2(a, v[0], v[1], v[2]);
+            p = X2C{v[0][0], v[0][1]};
+            s = X2C{v[1][0], v[1][1]};
+            i = X2C{v[2][0], v[2][1]};
+            return;
+        }
+        // corrected physics with a phase mismatch: per voxel
+        U *u[3] = {&p, &s, &i};
+        float2 w[2][3];
+#pragma unroll
+        for (int f = 0; f < 3; f++) {
+            const float2 re = f2unpack(u[f]->r), im = f2unpack(u[f]->i);
+            w[0][f] = float2{re.x, im.x};
+            w[1][f] = float2{re.y, im.y};
+        }
+        for (int h = 0; h < a.n_rk4; h++) {
+            rk4_half(a, h, w[0][0], w[0][1], w[0][2]);
+            rk4_half(a, h, w[1][0], w[1][1], w[1][2]);
+        }
+#pragma unroll
+        for (int f = 0; f < 3; f++) *u[f] = X2C{f2pack(float2{w[0][f].x, w[1][f].x}), f2pack(float2{w[0][f].y, w[1][f].y})};
+    }
 };
 
-template <int NT, int RA> struct LineItems {
-    static constexpr int A = LineGeom<NT, RA>::PP * LineGeom<NT, RA>::Q;  // RA-point butterflies per field
-    static constexpr int B = LineGeom<NT, RA>::PP * RA;                   // RB-point butterflies per field
+template <> struct LineUnit<double2> {
+    using U = double2;
+    static constexpr int PX = 1;
+    __device__ __forceinline__ static U lds(const void *p) { return *reinterpret_cast<const double2 *>(p); }
+    __device__ __forceinline__ static void sts(void *p, U v) { *reinterpret_cast<double2 *>(p) = v; }
+    __device__ __forceinline__ static U load_raw(const void *p) { return *reinterpret_cast<const double2 *>(p); }
+    __device__ __forceinline__ static void store_raw(void *p, U v) { *reinterpret_cast<double2 *>(p) = v; }
+    template <int R, int S> __device__ __forceinline__ static void dft(U *x) { opo::dft<R, S>(x); }
+    template <bool CONJ> __device__ __forceinline__ static U tmul(U x, double2 t) { return CONJ ? cmulc(x, t) : cmul(x, t); }
+    __device__ __forceinline__ static U zero() { return double2{0.0, 0.0}; }
+    __device__ __forceinline__ static void rk4(const TPassArgs<double2> &a, U &p, U &s, U &i)
+    {
+        for (int h = 0; h < a.n_rk4; h++) rk4_half(a, h, p, s, i);
+    }
 };
+
+template <typename C, int NT, int RA> struct LineGeom {
+    static constexpr int RB = NT / RA;
+    static constexpr int Q = RB;  // butterflies per line of the RA-point stage
+    static constexpr int PP = 4;  // units per row (time sample)
+    static constexpr int P = PP * LineUnit<C>::PX;  // pixels per tile
+    static constexpr int ROWS = NT + NT / RB;
+    static constexpr int REGION = ROWS * PP * 16;  // bytes per field region
+    static constexpr int A = PP * Q;   // RA-point butterflies per field
+    static constexpr int B = PP * RA;  // RB-point butterflies per field
+    __device__ __forceinline__ static constexpr int row(int t) { return t + t / RB; }
+    // byte offset of (field f, time sample t, unit u) in a tile buffer
+    __device__ __forceinline__ static constexpr int at(int f, int t, int u) { return f * REGION + (row(t) * PP + u) * 16; }
+    static constexpr int TILE_BYTES = 3 * REGION;
+    static constexpr size_t tile_bytes() { return (size_t)TILE_BYTES; }
+};
+
+// Issue the cp.async copies of tile `tile` (the fields in lmask) into buffer buf.
+template <typename C, int NT, int RA, int THREADS>
+__device__ __forceinline__ void line_stage_in(const TPassArgs<C> &a, unsigned tile, unsigned lmask, unsigned char *buf)
+{
+    using G = LineGeom<C, NT, RA>;
+    const unsigned base = tile_base(a.g, tile), gs = a.g.gs_j;
+    const C *src[3] = {a.psrc, a.f[1], a.f[2]};
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+        if (!(lmask & (1u << f))) continue;
+        const C *gsrc = src[f] + base;
+        for (unsigned e = threadIdx.x; e < NT * G::PP; e += THREADS) {
+            const int t = (int)(e / G::PP), u = (int)(e % G::PP);
+            cp_async<16>(buf + G::at(f, t, u), gsrc + (size_t)t * gs + u * LineUnit<C>::PX);
+        }
+    }
+}
+
+// Sweep over the staged tile: half steps and EOM per unit, two units per thread at a time
+// (items e and e + THREADS: two independent chains to interleave); transformed fields go
+// back to shared memory as units, the others (loaded, not transformed) to global memory.
+template <typename C, int NT, int RA, int THREADS>
+__device__ __forceinline__ void line_sweep(const TPassArgs<C> &a, unsigned base, unsigned lmask, unsigned tmask,
+                                           unsigned char *buf)
+{
+    using G = LineGeom<C, NT, RA>;
+    using L = LineUnit<C>;
+    using U = typename L::U;
+    const unsigned gs = a.g.gs_j;
+    auto load = [&](unsigned e, U (&v)[3]) {
+        const int t = (int)(e / G::PP), u = (int)(e % G::PP);
+#pragma unroll
+        for (int f = 0; f < 3; f++) v[f] = (lmask & (1u << f)) ? L::load_raw(buf + G::at(f, t, u)) : L::zero();
+    };
+    auto finish = [&](unsigned e, U (&v)[3]) {
+        const int t = (int)(e / G::PP), u = (int)(e % G::PP);
+        if (a.eom) {
+            const C ev = __ldg(a.eom + t);
+            v[1] = L::template tmul<false>(v[1], ev);
+            v[2] = L::template tmul<false>(v[2], ev);
+        }
+#pragma unroll
+        for (int f = 0; f < 3; f++) {
+            if (tmask & (1u << f))
+                L::sts(buf + G::at(f, t, u), v[f]);
+            else if (lmask & (1u << f))
+                L::store_raw(a.f[f] + base + (unsigned)t * gs + u * L::PX, v[f]);
+        }
+    };
+    constexpr unsigned NI = NT * G::PP;
+    for (unsigned e = threadIdx.x; e < NI; e += 2 * THREADS) {
+        const bool two = e + THREADS < NI;
+        U v0[3], v1[3];
+        load(e, v0);
+        if (two) load(e + THREADS, v1);
+        L::rk4(a, v0[0], v0[1], v0[2]);
+        if (two) L::rk4(a, v1[0], v1[1], v1[2]);
+        finish(e, v0);
+        if (two) finish(e + THREADS, v1);
+    }
+}
 
 // Item w of field f in the forward RA-point stage (stride Q): butterfly, then the
 // twiddles W_NT^{j k}.
-template <int NT, int RA>
-__device__ __forceinline__ void line_stage_a(const TPassArgs<float2> &a, float2 *sm, int f, int w)
+template <typename C, int NT, int RA>
+__device__ __forceinline__ void line_stage_a(const TPassArgs<C> &a, unsigned char *buf, int f, unsigned w)
 {
-    using G = LineGeom<NT, RA>;
-    constexpr int Q = G::Q, PP = G::PP;
-    const int pp = w % PP, j = w / PP;
-    float2 *sp = sm + f * G::REGION + 2 * pp;
-    X2C x[RA];
+    using G = LineGeom<C, NT, RA>;
+    using L = LineUnit<C>;
+    constexpr int Q = G::Q;
+    const int u = (int)(w % G::PP), j = (int)(w / G::PP);
+    typename L::U x[RA];
 #pragma unroll
-    for (int m = 0; m < RA; m++) x[m] = lds_x2c(sp + G::row(j + Q * m) * kLineP);
-    xdft<RA, +1>(x);
+    for (int m = 0; m < RA; m++) x[m] = L::lds(buf + G::at(f, j + Q * m, u));
+    L::template dft<RA, +1>(x);
 #pragma unroll
-    for (int k = 1; k < RA; k++) x[k] = xmul_tab<true>(x[k], __ldg(a.tw + (k - 1) * Q + j));
+    for (int k = 1; k < RA; k++) x[k] = L::template tmul<true>(x[k], __ldg(a.tw + (k - 1) * Q + j));
 #pragma unroll
-    for (int k = 0; k < RA; k++) sts_x2c(sp + G::row(j + Q * k) * kLineP, x[k]);
+    for (int k = 0; k < RA; k++) L::sts(buf + G::at(f, j + Q * k, u), x[k]);
 }
 
 // Item w of field f in the RB-point stage: butterfly, phase table, inverse butterfly.
-template <int NT, int RA>
-__device__ __forceinline__ void line_stage_b(const TPassArgs<float2> &a, float2 *sm, int f, int w)
+template <typename C, int NT, int RA>
+__device__ __forceinline__ void line_stage_b(const TPassArgs<C> &a, unsigned char *buf, int f, unsigned w)
 {
-    using G = LineGeom<NT, RA>;
-    constexpr int RB = G::RB, PP = G::PP;
-    const int pp = w % PP, g = w / PP;
-    float2 *sp = sm + f * G::REGION + G::row(RB * g) * kLineP + 2 * pp;
-    const float2 *tb = a.tab[f] + RB * g;
-    X2C x[RB];
+    using G = LineGeom<C, NT, RA>;
+    using L = LineUnit<C>;
+    constexpr int RB = G::RB;
+    const int u = (int)(w % G::PP), g = (int)(w / G::PP);
+    unsigned char *sp = buf + G::at(f, RB * g, u);
+    const C *tb = a.tab[f] + RB * g;
+    typename L::U x[RB];
 #pragma unroll
-    for (int m = 0; m < RB; m++) x[m] = lds_x2c(sp + m * kLineP);
-    xdft<RB, +1>(x);
+    for (int m = 0; m < RB; m++) x[m] = L::lds(sp + m * G::PP * 16);
+    L::template dft<RB, +1>(x);
+    if constexpr (sizeof(C) == 8) {
+        // two FP32 table entries per 16-byte load (tb is 16-byte aligned: RB g even)
 #pragma unroll
-    for (int k = 0; k < RB; k++) x[k] = xmul_tab<false>(x[k], __ldg(tb + k));
-    xdft<RB, -1>(x);
+        for (int k = 0; k < RB; k += 2) {
+            const float4 t2 = __ldg(reinterpret_cast<const float4 *>(tb + k));
+            x[k] = L::template tmul<false>(x[k], C{t2.x, t2.y});
+            x[k + 1] = L::template tmul<false>(x[k + 1], C{t2.z, t2.w});
+        }
+    } else {
 #pragma unroll
-    for (int k = 0; k < RB; k++) sts_x2c(sp + k * kLineP, x[k]);
+        for (int k = 0; k < RB; k++) x[k] = L::template tmul<false>(x[k], __ldg(tb + k));
+    }
+    L::template dft<RB, -1>(x);
+#pragma unroll
+    for (int k = 0; k < RB; k++) L::sts(sp + k * G::PP * 16, x[k]);
 }
 
 // Item w of field f in the inverse RA-point stage (twiddles before the butterfly),
 // written to global memory.
-template <int NT, int RA>
-__device__ __forceinline__ void line_stage_c(const TPassArgs<float2> &a, const float2 *sm, int f, int w,
+template <typename C, int NT, int RA>
+__device__ __forceinline__ void line_stage_c(const TPassArgs<C> &a, const unsigned char *buf, int f, unsigned w,
                                              unsigned base, unsigned gs)
 {
-    using G = LineGeom<NT, RA>;
-    constexpr int Q = G::Q, PP = G::PP;
-    const int pp = w % PP, j = w / PP;
-    const float2 *sp = sm + f * G::REGION + 2 * pp;
-    X2C x[RA];
+    using G = LineGeom<C, NT, RA>;
+    using L = LineUnit<C>;
+    constexpr int Q = G::Q;
+    const int u = (int)(w % G::PP), j = (int)(w / G::PP);
+    typename L::U x[RA];
 #pragma unroll
-    for (int m = 0; m < RA; m++) x[m] = lds_x2c(sp + G::row(j + Q * m) * kLineP);
+    for (int m = 0; m < RA; m++) x[m] = L::lds(buf + G::at(f, j + Q * m, u));
 #pragma unroll
-    for (int m = 1; m < RA; m++) x[m] = xmul_tab<false>(x[m], __ldg(a.tw + (m - 1) * Q + j));
-    xdft<RA, -1>(x);
-    float2 *d = a.f[f] + base + (unsigned)j * gs + 2 * pp;
+    for (int m = 1; m < RA; m++) x[m] = L::template tmul<false>(x[m], __ldg(a.tw + (m - 1) * Q + j));
+    L::template dft<RA, -1>(x);
+    C *d = a.f[f] + base + (unsigned)j * gs + u * L::PX;
 #pragma unroll
-    for (int k = 0; k < RA; k++) *reinterpret_cast<float4 *>(d + (size_t)(Q * k) * gs) = interleaved_of(x[k]);
+    for (int k = 0; k < RA; k++) L::store_raw(d + (size_t)(Q * k) * gs, x[k]);
 }
 
-// One tile: P = 8 consecutive pixels of one row, all NT samples, the fields in the load
-// mask, staged with cp.async; coupled-wave half steps (and the EOM) as a sweep over the
-// tile; then per transformed field the RA-point stage, the fused RB-point stage with the
-// phase table, and the inverse RA-point stage written to global memory.
-template <int NT, int RA, int THREADS, int BAR = 0>
-__device__ __forceinline__ void tpass_line_tile(const TPassArgs<float2> &a, unsigned tile, float2 *sm)
+// The three transform stages of every field in tmask as jobs (stage, field) in
+// stage-major order, two jobs per phase (half the CTA each; one job when one field is
+// transformed) and a CTA barrier between phases.  A job's stage of a field always ran
+// in an earlier phase (nf >= 2 jobs apart), and three fields take five phases of whole
+// warps instead of three stages that leave half the warps idle for their second half.
+template <typename C, int NT, int RA, int THREADS, int BAR, int PER>
+__device__ __forceinline__ void line_jobs(const TPassArgs<C> &a, unsigned base, unsigned tmask, unsigned nf,
+                                          unsigned char *buf)
 {
-    using G = LineGeom<NT, RA>;
-    constexpr int PP = G::PP;
+    using G = LineGeom<C, NT, RA>;
+    constexpr unsigned GROUP = THREADS / PER;
+    const unsigned gs = a.g.gs_j, njobs = 3 * nf;
+    const unsigned slot = threadIdx.x / GROUP, w0 = threadIdx.x % GROUP;
+    for (unsigned j0 = 0; j0 < njobs; j0 += PER) {
+        const unsigned j = j0 + slot;
+        if (j < njobs) {
+            // stage j / nf and field j % nf for nf = 1, 2, 3 (j < 9: j / 3 = (11 j) >> 5)
+            const unsigned stage = nf == 1 ? j : (nf == 2 ? j >> 1 : (11 * j) >> 5);
+            const int f = field_id(tmask, (int)(j - stage * nf));
+            if (stage == 0) {
+                for (unsigned w = w0; w < G::A; w += GROUP) line_stage_a<C, NT, RA>(a, buf, f, w);
+            } else if (stage == 1) {
+                for (unsigned w = w0; w < G::B; w += GROUP) line_stage_b<C, NT, RA>(a, buf, f, w);
+            } else {
+                for (unsigned w = w0; w < G::A; w += GROUP) line_stage_c<C, NT, RA>(a, buf, f, w, base, gs);
+            }
+        }
+        tile_sync<BAR>();
+    }
+}
+
+template <typename C, int NT, int RA, int THREADS, int BAR>
+__device__ __forceinline__ void line_transforms(const TPassArgs<C> &a, unsigned base, unsigned tmask, unsigned char *buf)
+{
+    const unsigned nf = __popc(tmask);
+    if (nf >= 2)
+        line_jobs<C, NT, RA, THREADS, BAR, 2>(a, base, tmask, nf, buf);
+    else
+        line_jobs<C, NT, RA, THREADS, BAR, 1>(a, base, tmask, nf, buf);
+}
+
+// One tile: the fields in the load mask staged with cp.async, the sweep, then per
+// transformed field the RA-point stage, the fused RB-point stage with the phase table,
+// and the inverse RA-point stage written to global memory.  Ends with the CTA
+// synchronised.
+template <typename C, int NT, int RA, int THREADS, int BAR = 0>
+__device__ __forceinline__ void tpass_line_tile(const TPassArgs<C> &a, unsigned tile, unsigned char *buf)
+{
     const unsigned base = tile_base(a.g, tile);
-    const unsigned gs = a.g.gs_j;  // nx ny: one time sample
-    const unsigned tmask = a.tmask;
-    const unsigned lmask = tpass_load_mask(a);
-
-    // stage the tile: 16-byte copies of pixel pairs, interleaved as in global memory
-    {
-        const float2 *src[3] = {a.psrc, a.f[1], a.f[2]};
-#pragma unroll
-        for (int f = 0; f < 3; f++) {
-            if (!(lmask & (1u << f))) continue;
-            const float2 *gsrc = src[f] + base;
-            float2 *dst = sm + f * G::REGION;
-            for (int e = threadIdx.x; e < NT * PP; e += THREADS) {
-                const int t = e / PP, pp = e % PP;
-                cp_async<16>(dst + G::row(t) * kLineP + 2 * pp, gsrc + (size_t)t * gs + 2 * pp);
-            }
-        }
-        cp_async_wait_all();
-        tile_sync<BAR>();
-    }
-
-    // sweep: half steps and EOM per voxel pair; transformed fields go back to shared
-    // memory as split pairs, the others (loaded, not transformed) to global memory
-    for (int e = threadIdx.x; e < NT * PP; e += THREADS) {
-        const int t = e / PP, pp = e % PP;
-        const int off = G::row(t) * kLineP + 2 * pp;
-        f32x2 v[3][2];
-#pragma unroll
-        for (int f = 0; f < 3; f++) {
-            float4 q4 = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (lmask & (1u << f)) q4 = *reinterpret_cast<const float4 *>(sm + f * G::REGION + off);
-            const X2C x = split_of(q4);
-            v[f][0] = x.r;
-            v[f][1] = x.i;
-        }
-        if (!a.use_phase) {
-            for (int h = 0; h < a.n_rk4; h++) rk4_half_fast_x2(a, v[0], v[1], v[2]);
-        } else if (a.n_rk4 > 0) {
-            // corrected physics with a phase mismatch: per voxel
-            float2 u[2][3];
-#pragma unroll
-            for (int f = 0; f < 3; f++) {
-                const float2 re = f2unpack(v[f][0]), im = f2unpack(v[f][1]);
-                u[0][f] = float2{re.x, im.x};
-                u[1][f] = float2{re.y, im.y};
-            }
-            for (int h = 0; h < a.n_rk4; h++) {
-                rk4_half(a, h, u[0][0], u[0][1], u[0][2]);
-                rk4_half(a, h, u[1][0], u[1][1], u[1][2]);
-            }
-#pragma unroll
-            for (int f = 0; f < 3; f++) {
-                v[f][0] = f2pack(float2{u[0][f].x, u[1][f].x});
-                v[f][1] = f2pack(float2{u[0][f].y, u[1][f].y});
-            }
-        }
-        if (a.eom) {
-            const float2 ev = __ldg(a.eom + t);
-            const f32x2 er = x2_dup(ev.x), ei = x2_dup(ev.y), nei = x2_dup(-ev.y);
-#pragma unroll
-            for (int f = 1; f < 3; f++) {
-                const X2C y = xmul(X2C{v[f][0], v[f][1]}, er, ei, nei);
-                v[f][0] = y.r;
-                v[f][1] = y.i;
-            }
-        }
-        const unsigned gb = base + (unsigned)t * gs + 2 * pp;
-#pragma unroll
-        for (int f = 0; f < 3; f++) {
-            if (tmask & (1u << f))
-                sts_x2c(sm + f * G::REGION + off, X2C{v[f][0], v[f][1]});
-            else if (lmask & (1u << f))
-                *reinterpret_cast<float4 *>(a.f[f] + gb) = interleaved_of(X2C{v[f][0], v[f][1]});
-        }
-    }
-    if (!tmask) {
-        tile_sync<BAR>();
-        return;
-    }
+    const unsigned tmask = a.tmask, lmask = tpass_load_mask(a);
+    line_stage_in<C, NT, RA, THREADS>(a, tile, lmask, buf);
+    cp_async_wait_all();
     tile_sync<BAR>();
-    const int nf = __popc(tmask);
-    if constexpr (THREADS == 32 * 3) {
-        // one warp per transformed field: its three stages synchronise the warp only
-        const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if (wid < nf) {
-            const int f = field_id(tmask, wid);
-#pragma unroll
-            for (int w = lane; w < LineItems<NT, RA>::A; w += 32) line_stage_a<NT, RA>(a, sm, f, w);
-            __syncwarp();
-#pragma unroll
-            for (int w = lane; w < LineItems<NT, RA>::B; w += 32) line_stage_b<NT, RA>(a, sm, f, w);
-            __syncwarp();
-#pragma unroll
-            for (int w = lane; w < LineItems<NT, RA>::A; w += 32) line_stage_c<NT, RA>(a, sm, f, w, base, gs);
-        }
-    } else {
-        constexpr int IA = LineItems<NT, RA>::A, IB = LineItems<NT, RA>::B;
-        for (int u = threadIdx.x; u < nf * IA; u += THREADS) line_stage_a<NT, RA>(a, sm, field_id(tmask, u / IA), u % IA);
-        tile_sync<BAR>();
-        for (int u = threadIdx.x; u < nf * IB; u += THREADS) line_stage_b<NT, RA>(a, sm, field_id(tmask, u / IB), u % IB);
-        tile_sync<BAR>();
-        for (int u = threadIdx.x; u < nf * IA; u += THREADS)
-            line_stage_c<NT, RA>(a, sm, field_id(tmask, u / IA), u % IA, base, gs);
-    }
+    line_sweep<C, NT, RA, THREADS>(a, base, lmask, tmask, buf);
     tile_sync<BAR>();
+    if (tmask) line_transforms<C, NT, RA, THREADS, BAR>(a, base, tmask, buf);
 }
 
 }  // namespace opo

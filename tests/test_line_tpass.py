@@ -1,8 +1,8 @@
-"""Line-specialised FP32 t-pass (tuning r1 + co.LINE): compile-time time axes 64, 128
-and 256, tiles of 8 pixels, two pixels per packed f32x2 instruction.  It must match the
-FP64 oracle within the precision form's 1e-5 (round trips with GDD, mirrors, EOM, the
-corrected physics with a phase mismatch, the closing pass's untransformed pump), agree
-with the generic FP32 kernel of the same radix to FP32 rounding, fall back to the generic
+"""Line-specialised t-pass (tuning r1 + co.LINE): compile-time time axes 64, 128 and 256,
+tiles of 8 FP32 pixels (two per packed f32x2 instruction) or 4 FP64 pixels.  It must match
+the FP64 oracle within the form's tolerance (FP32 1e-5, FP64 1e-10; round trips with GDD,
+mirrors, EOM, the corrected physics with a phase mismatch, the closing pass's
+untransformed pump), agree with the generic kernel to rounding, fall back to the generic
 kernel on grids it does not cover, and give bit-identical results in a batch and in a
 standalone solver (the batched kernel runs the same tile body per instance)."""
 import numpy as np
@@ -14,15 +14,17 @@ from oracle import pyoracle as po
 
 pytestmark = pytest.mark.gpu
 
-FP32_TOL = 1e-5
+TOL = {co.FP32: 1e-5, co.FP64: 1e-10}
+# against the generic kernel: FP32 / FP64 rounding apart
+GEN_TOL = {co.FP32: 2e-6, co.FP64: 1e-12}
 AXES = {"x": dict(threads=128, tile=1024, r1=8), "y": dict(threads=128, tile=1024, r1=8)}
 
 
-def tuning(r1, line=True, nt=256, threads=128):
-    return {"t": dict(threads=threads, tile=max(nt * 8, 1024), r1=r1 + (co.LINE if line else 0)), **AXES}
+def tuning(r1, line=True, nt=256):
+    return {"t": dict(threads=128, tile=max(nt * 8, 1024), r1=r1 + (co.LINE if line else 0)), **AXES}
 
 
-def run(grid, over, tun, nrt=2, precision=co.FP32, seed=31):
+def run(grid, over, tun, precision, nrt=2, seed=31):
     nx, ny, nt = grid
     kw = dict(nx=nx, ny=ny, nt=nt, nz=4, LX=300.0, LY=250.0, Lcr=3000.0, P=400.0, w0=40.0, FWHM=3.0, t_window=25.0,
               pump_mode="focused-pulsed", gdd_gamma=0.6, Rs=0.9, total_rt=3, **over)
@@ -44,6 +46,12 @@ def run(grid, over, tun, nrt=2, precision=co.FP32, seed=31):
     return out, kw, flags, s0, t
 
 
+def oracle(kw, flags, s0, nrt=2):
+    st = po.Setup(po.make_phys(flags=flags, **kw))
+    api = st.api_complex()
+    return po.round_trips(st, api, api, s0, s0, nrt)
+
+
 LINE_CASES = [
     ((32, 32, 256), 16, {}),
     ((16, 8, 128), 16, dict(eom_beta=0.4, eom_fpm=0.05)),
@@ -53,85 +61,88 @@ LINE_CASES = [
 ]
 
 
-@pytest.mark.parametrize("threads", [128, 96])
+@pytest.mark.parametrize("precision", [co.FP32, co.FP64])
 @pytest.mark.parametrize("grid,r1,over", LINE_CASES)
-def test_line_tpass_vs_oracle_and_generic(grid, r1, over, threads):
-    """128-thread CTAs spread every field's butterflies over the CTA; 96-thread CTAs give
-    each transformed field one warp."""
-    out, kw, flags, s0, t = run(grid, over, tuning(r1, nt=grid[2], threads=threads))
-    assert t["r1"] == r1 + co.LINE and t["threads"] == threads
-    st = po.Setup(po.make_phys(flags=flags, **kw))
-    api = st.api_complex()
-    ref = po.round_trips(st, api, api, s0, s0, 2)
-    for a, b in zip(out, ref):
-        assert rel_l2(a, b) < FP32_TOL
-    # the generic kernel of the same radix: the same arithmetic up to FP32 rounding, but
-    # not bit for bit (so the line kernel is the one that ran)
-    gen, *_ = run(grid, over, tuning(r1, line=False, nt=grid[2]))
+def test_line_tpass_vs_oracle_and_generic(grid, r1, over, precision):
+    out, kw, flags, s0, t = run(grid, over, tuning(r1, nt=grid[2]), precision)
+    assert t["r1"] == r1 + co.LINE
+    for a, b in zip(out, oracle(kw, flags, s0)):
+        assert rel_l2(a, b) < TOL[precision]
+    # the generic kernel (FP64: its radix-4 register form): the same arithmetic up to
+    # rounding, but not bit for bit (so the line kernel is the one that ran)
+    gen, *_ = run(grid, over, tuning(4 if precision == co.FP64 else r1, line=False, nt=grid[2]), precision)
     diff = [rel_l2(a, b) for a, b in zip(out, gen)]
-    assert max(diff) < 2e-6, diff
+    assert max(diff) < GEN_TOL[precision], diff
     assert any(not np.array_equal(a, b) for a, b in zip(out, gen))
 
 
-@pytest.mark.parametrize("grid,over", [((16, 8, 96), {}), ((12, 8, 128), {}),
+@pytest.mark.parametrize("precision", [co.FP32, co.FP64])
+@pytest.mark.parametrize("grid,over", [((16, 8, 96), {}), ((6, 8, 128), dict(flags=co.DISPERSION)),
                                        ((16, 16, 256), dict(flags=co.DISPERSION | co.DIFFRACTION | co.ASIS_Q2))])
-def test_line_tuning_falls_back_to_generic_kernel(grid, over):
-    """Grids without a line body (time axis 96, nx not a multiple of 8, the shipped Q2
-    launch grid) keep the line setting but run the generic tile body: bit for bit the
-    generic kernel's results (128 threads); with 96 threads, the oracle's within 1e-5."""
-    out, kw, flags, s0, t = run(grid, over, tuning(16, nt=grid[2], threads=96))
-    assert t["r1"] & co.LINE and t["threads"] == 96
-    st = po.Setup(po.make_phys(flags=flags, **kw))
-    api = st.api_complex()
-    ref = po.round_trips(st, api, api, s0, s0, 2)
-    for a, b in zip(out, ref):
-        assert rel_l2(a, b) < FP32_TOL
-    out, _, _, _, t = run(grid, over, tuning(16, nt=grid[2]))
+def test_line_tuning_falls_back_to_generic_kernel(grid, over, precision):
+    """Grids without a line body (time axis 96, nx = 6 not a multiple of the tile, the
+    shipped Q2 launch grid) keep the line setting but run the generic tile body (FP64: its radix-4
+    register form): bit for bit the generic kernel's results, and the oracle's within the
+    form's tolerance."""
+    out, kw, flags, s0, t = run(grid, over, tuning(16, nt=grid[2]), precision)
     assert t["r1"] & co.LINE
-    gen, *_ = run(grid, over, tuning(t["r1"] - co.LINE, line=False, nt=grid[2]))
+    for a, b in zip(out, oracle(kw, flags, s0)):
+        assert rel_l2(a, b) < TOL[precision]
+    gen, *_ = run(grid, over, tuning(t["r1"] - co.LINE, line=False, nt=grid[2]), precision)
     for a, b in zip(out, gen):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("threads", [128, 96])
-def test_line_tpass_full_size_vs_fp64(threads):
+def test_line_tpass_full_size_vs_fp64():
     """128 x 128 x 256, the benchmark's physics, one full round trip (100 z-steps): the
-    line-specialised FP32 t-pass within 1e-5 of the FP64 form."""
+    FP32 line t-pass within 1e-5 of the FP64 line t-pass, which is within 1e-12 of the
+    generic FP64 kernels."""
     kw = dict(nx=128, ny=128, nt=256, nz=100, LX=800.0, LY=800.0, Lcr=20000.0, t_window=40.0, P=5.0,
               w0=60.0, FWHM=2.0, Rs=0.98, alpha=(-1.0, 2e-7, 2e-7), pump_mode="focused-pulsed",
               gdd_gamma=1.0, total_rt=200)
+    tunings = {"fp32": (co.FP32, {"t": dict(threads=128, tile=2048, r1=16 + co.LINE),
+                                  "x": dict(threads=128, tile=2048, r1=8), "y": dict(threads=128, tile=2048, r1=16)}),
+               "fp64": (co.FP64, {"t": dict(threads=128, tile=1024, r1=16 + co.LINE),
+                                  "x": dict(threads=160, tile=1024, r1=8), "y": dict(threads=160, tile=1024, r1=8)}),
+               "fp64_generic": (co.FP64, {"t": dict(threads=128, tile=1024, r1=4),
+                                          "x": dict(threads=160, tile=1024, r1=8),
+                                          "y": dict(threads=160, tile=1024, r1=8)})}
     outs = {}
-    for prec in (co.FP64, co.FP32):
+    for name, (prec, tun) in tunings.items():
         cfg = co.make_config(precision=prec, **kw)
         params, _ = co.derive(cfg)
         _, w = co.time_freq(cfg.nt, params.t_window)
         sim = co.Simulation(params, w)
-        if prec == co.FP32:
-            sim.set_tuning({"t": dict(threads=threads, tile=2048, r1=16 + co.LINE),
-                            "x": dict(threads=128, tile=2048, r1=8), "y": dict(threads=128, tile=2048, r1=16)})
-            assert sim.tuning["t"]["r1"] == 16 + co.LINE
+        sim.set_tuning(tun)
+        assert sim.tuning["t"]["r1"] == tun["t"]["r1"]
         sim.init_fields(cfg, 1, 1e-3, idler_copy=True)
         sim.run_round_trips(1)
-        outs[prec] = [sim.get_field(k) for k in (co.FIELD_AP, co.FIELD_AS, co.FIELD_AI)]
+        outs[name] = [sim.get_field(k) for k in (co.FIELD_AP, co.FIELD_AS, co.FIELD_AI)]
         sim.close()
-    for a, b in zip(outs[co.FP32], outs[co.FP64]):
-        assert rel_l2(a, b) < FP32_TOL
+    for a, b, c in zip(outs["fp32"], outs["fp64"], outs["fp64_generic"]):
+        assert rel_l2(a, b) < TOL[co.FP32]
+        assert rel_l2(b, c) < 1e-12
 
 
-@pytest.mark.parametrize("threads", [128, 96])
-def test_line_tpass_batch_equals_standalone(threads):
-    """A batch tuned to the line form, with instances on line axes (256, 128) and one
-    without (96, generic body in the same launch): every slot bit for bit its standalone
-    solver."""
+@pytest.mark.parametrize("precision", [co.FP32, co.FP64])
+def test_line_tpass_batch_equals_standalone(precision):
+    """A batch tuned to the line form, with instances on line axes (256, 128) and, in FP32,
+    one without (96: the generic body in the same launch; an FP64 instance without a line
+    body takes radix 4 and is refused): every slot bit for bit its standalone solver."""
     base = dict(nz=4, LX=300.0, LY=300.0, Lcr=3000.0, FWHM=3.0, t_window=25.0, pump_mode="focused-pulsed",
-                total_rt=3, precision=co.FP32)
+                total_rt=3, precision=precision)
     insts = [dict(nx=16, ny=16, nt=256, P=300.0, w0=40.0, gdd_gamma=1.0),
              dict(nx=32, ny=16, nt=128, P=150.0, w0=60.0, detuning=0.7, Rs=0.9),
-             dict(nx=16, ny=16, nt=96, P=500.0, w0=35.0, detuning=-1.2),
              dict(nx=24, ny=24, nt=128, P=80.0, w0=50.0, flags=co.DISPERSION | co.DIFFRACTION | co.PHYSICS,
                   Lambda=6.5)]
-    tun = {"t": dict(threads=threads, tile=2048, r1=16 + co.LINE), **AXES}
-    b = co.Batch(co.FP32, 8, 8 << 30, tuning=tun)
+    other = dict(nx=16, ny=16, nt=96, P=500.0, w0=35.0, detuning=-1.2)
+    tun = {"t": dict(threads=128, tile=2048, r1=16 + co.LINE), **AXES}
+    b = co.Batch(precision, 8, 8 << 30, tuning=tun)
+    if precision == co.FP32:
+        insts.append(other)
+    else:
+        with pytest.raises(co.OpoError):
+            b.add(co.make_config(**{**base, **other}))
     slots = []
     for k, inst in enumerate(insts):
         cfg = co.make_config(**{**base, **inst})
