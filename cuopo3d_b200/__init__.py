@@ -22,7 +22,7 @@ OPO_ERR_COURANT, OPO_ERR_CAPACITY = 5, 6
 # flags
 DISPERSION, DIFFRACTION, PHYSICS, ASIS_Q1, ASIS_Q2, TOD = 1, 2, 4, 8, 16, 32
 FP32, FP64 = 0, 1
-# added to a t-pass "r1" in a tuning: the line-specialised FP32 t-pass (OPO_TUNE_LINE)
+# added to a t-pass "r1" in a tuning: the line-specialised t-pass (OPO_TUNE_LINE)
 LINE = 256
 PPLN_ID, MGOSPPLT_ID, MGOPPLN_ID, ZGP_ID = 0, 1, 2, 3
 CRYSTALS = {"ppln": PPLN_ID, "mgospplt": MGOSPPLT_ID, "mgosplt": MGOSPPLT_ID, "mgoppln": MGOPPLN_ID,
