@@ -79,12 +79,11 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 4 : 1)
     }
 }
 
-// Batched line-specialised t-pass: instances whose grid has a line form (line_nt) run
-// that body (one tile at a time, one tile buffer), the others (FP32 only) the generic
-// body of the same CTA size and first-stage radix.  An FP64 instance without a line body
-// takes radix 4 and is refused by a batch of this variant, so FP64 needs no fallback.
-template <typename C, int R1, int THREADS>
-__global__ void __launch_bounds__(THREADS, 4)
+// Batched line-specialised t-pass: instances whose grid has a line body (line_nt: 256,
+// 128, 64) run it (one tile at a time, one tile buffer), the others the generic body of
+// the same CTA size with the setting's fallback radix RF.
+template <typename C, int RF, int THREADS>
+__global__ void __launch_bounds__(THREADS, 3)
     tpass_line_batch_kernel(const TPassArgs<C> *descs, const unsigned *prefix, const BatchHeader *hdr, int tp)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -103,17 +102,17 @@ __global__ void __launch_bounds__(THREADS, 4)
             cur = i;
         }
         const unsigned tile = gt - __ldg(prefix + i);
-        if (R1 == 16 && d->line_nt == 256) {
-            if constexpr (R1 == 16) tpass_line_tile<C, 256, 16, THREADS>(*d, tile, buf);
-        } else if (R1 == 16 && d->line_nt == 128) {
-            if constexpr (R1 == 16) tpass_line_tile<C, 128, 16, THREADS>(*d, tile, buf);
-        } else if (R1 == 8 && d->line_nt == 64) {
-            if constexpr (R1 == 8) tpass_line_tile<C, 64, 8, THREADS>(*d, tile, buf);
-        } else if constexpr (sizeof(C) == 8) {
+        if (d->line_nt == 256) {
+            tpass_line_tile<C, 256, 16, THREADS>(*d, tile, buf);
+        } else if (d->line_nt == 128) {
+            tpass_line_tile<C, 128, 16, THREADS>(*d, tile, buf);
+        } else if (d->line_nt == 64) {
+            tpass_line_tile<C, 64, 8, THREADS>(*d, tile, buf);
+        } else {
             C *sm = reinterpret_cast<C *>(buf);
             const C *src[3] = {d->psrc, d->f[1], d->f[2]};
             stage_tile<C, THREADS, false>(d->g, (unsigned)d->plan.n, tile, src, tpass_load_mask(*d), sm);
-            tpass_tile<C, R1, THREADS, 16, true>(*d, tile, sm);
+            tpass_tile<C, RF, THREADS, LineFallback<C, THREADS>::RMAX, true>(*d, tile, sm);
         }
     }
 }
@@ -206,8 +205,14 @@ template <typename C> bool batch_t_func(PassVariant v, const void **fn)
 {
     if (is_line(v)) {
         if (!line_variant_compiled(v.threads, radix_of(v))) return false;
-        *fn = radix_of(v) == 16 ? reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 16, 128>)
-                                : reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 8, 128>);
+        if constexpr (sizeof(C) == 16) {
+            *fn = reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 4, 128>);
+        } else {
+            const int rf = line_fallback_radix(false, v);
+            *fn = rf == 16  ? reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 16, 128>)
+                  : rf == 8 ? reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 8, 128>)
+                            : reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 4, 128>);
+        }
         return true;
     }
     bool ok = false;
@@ -632,7 +637,7 @@ int opo_batch_add(OpoBatch *b, const OpoParams *p, const double *w, int *slot_ou
     if (rc) return bfail(b, rc, "instance creation failed (grid not supported by the batch's kernel variants?)");
     for (int k = 0; k < 3; k++) {
         const opo::PassVariant got = opo::solver_pass_variant(s, k);
-        if (got.r1 != b->v[k].r1 || got.threads != b->v[k].threads) {
+        if (got.r1 != b->v[k].r1 || got.threads != b->v[k].threads || (k == 0 && !opo::solver_line_fallback_ok(s))) {
             opo_destroy(s);
             return bfail(b, OPO_ERR_INVALID, "grid needs a first-stage radix other than the batch's");
         }

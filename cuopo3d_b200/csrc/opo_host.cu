@@ -567,15 +567,19 @@ template <typename C> int configure_pass(OpoSolver *s, int kind, opo::PassVarian
     const int form = v.r1 & opo::kLineForm;
     int r1 = opo::radix_of(v);
     // line-specialised t-pass: a compiled time axis with its two-stage plan, whole tiles of
-    // line_pixels() pixels, and every pixel transformed (not the shipped Q2 launch grid)
+    // line_pixels() pixels, and every pixel transformed (not the shipped Q2 launch grid);
+    // otherwise its generic fallback radix
     const int LP = opo::line_pixels(fp64);
-    const bool line = form && kind == kT && opo::line_shape(nt, r1) && nx % LP == 0 && !(p.flags & OPO_ASIS_Q2);
-    // 3 fields x r1 complex128 live in registers (the line form's generic fallback: radix 4)
-    if (fp64 && kind == kT && !line) r1 = std::min(r1, form ? 4 : 8);
+    const bool line = form && kind == kT && opo::line_radix(nt) && nx % LP == 0 && !(p.flags & OPO_ASIS_Q2);
+    if (line) r1 = opo::line_radix(nt);
+    else if (form) r1 = opo::line_fallback_radix(fp64, v);
+    else if (fp64 && kind == kT) r1 = std::min(r1, 8);  // 3 fields x r1 complex128 live in registers
     while (r1 >= 4 && !build_plan(n, r1, line ? 16 : opo::variant_max_radix(fp64, v), pc.plan, tw)) r1 /= 2;
     if (r1 < 4) return fail(s, OPO_ERR_INVALID, "grid sizes must be 2^a 3^b and >= 8");
-    pc.v.r1 = r1 | form;
-    if (line && pc.plan.ns == 2 && r1 == opo::radix_of(v)) pc.line_nt = nt;
+    // a line variant keeps its setting (the bodies fix their radices); the fallback's
+    // radix is checked by batches (solver_line_fallback_ok)
+    pc.v.r1 = form ? v.r1 : r1;
+    if (line && pc.plan.ns == 2) pc.line_nt = nt;
     const unsigned nxy = (unsigned)nx * ny;
     opo::TileGeom &g = pc.geo;
     if (pc.line_nt) {
@@ -954,7 +958,8 @@ int enqueue_t(OpoSolver *s, bool reset_pump, int n_rk4, const double *zh, int wh
                                           s->stream),
                "t-pass launch");
     } else if (opo::is_line(pc.v)) {
-        OPO_CU(s, opo::launch_tpass_line<C>(a, pc.v, pc.line_nt, pc.grid, pc.smem, s->stream), "t-pass launch");
+        OPO_CU(s, opo::launch_tpass_line<C>(a, pc.v, pc.line_nt, pc.plan.radix[0], pc.grid, pc.smem, s->stream),
+               "t-pass launch");
     } else {
         OPO_CU(s, opo::launch_tpass<C>(a, opo::PassVariant{pc.v.threads, opo::radix_of(pc.v)}, pc.grid, pc.smem,
                                        s->stream),
@@ -1272,7 +1277,9 @@ template <typename C> int autotune(OpoSolver *s)
         // line-specialised FP32 t-pass variants, where the grid has a compiled form
         for (int r1 : r1s) {
             const opo::PassVariant lv{128, r1 | opo::kLineForm};
-            if (kind != kT || !opo::variant_compiled(fp64, true, lv)) continue;
+            // one candidate per precision: its fallback radix (FP32 16, FP64 4) only matters
+            // on grids without a line body
+            if (kind != kT || !opo::variant_compiled(fp64, true, lv) || r1 != (fp64 ? 4 : 16)) continue;
             if (configure_pass<C>(s, kind, lv, tes[0]) != OPO_OK || !s->pass[kind].line_nt) continue;
             float ms = 0;
             int rc = time_pass<C>(s, kind, &ms);
@@ -1857,6 +1864,13 @@ int solver_create_configured(const OpoParams *p, const double *w, const PassVari
 }
 
 PassVariant solver_pass_variant(const OpoSolver *s, int kind) { return s->pass[kind].v; }
+
+bool solver_line_fallback_ok(const OpoSolver *s)
+{
+    const PassCfg &pc = s->pass[kT];
+    if (!is_line(pc.v) || pc.line_nt) return true;
+    return pc.plan.radix[0] == line_fallback_radix(s->p.precision == OPO_FP64, pc.v);
+}
 
 void solver_pass_info(const OpoSolver *s, int kind, int *ntiles, size_t *smem)
 {

@@ -154,27 +154,29 @@ struct WsArgs {
 // stage may use follows from the precision and CTA size (max_radix()).
 struct PassVariant {
     int threads;  // 128 or 256; 160 or 288: warp-specialised (128 / 256 consumers + a producer warp)
-    int r1;       // 4, 8 or 16, plus kLineForm for the line-specialised FP32 t-pass
+    int r1;       // 4, 8 or 16, plus kLineForm for the line-specialised t-pass
 };
 
 // Flag in PassVariant::r1 (and in the r1 entries of the C-ABI tuning arrays): the
-// line-specialised t-pass (tpass_line.cuh: compile-time time axis 64, 128 or 256, tiles
-// of 8 FP32 or 4 FP64 pixels, FP32 split-pair arithmetic) with the given first-stage
-// radix, on CTAs of 128 threads.  Grids it does not cover (another time axis, nx not a
-// multiple of the tile, the shipped Q2 launch grid) run the generic tile body at the
-// same CTA size and radix (FP64: radix 4) instead.
+// line-specialised t-pass (tpass_line.cuh: tiles of 8 FP32 or 4 FP64 pixels, FP32
+// split-pair arithmetic) on CTAs of 128 threads, for every time axis with a compiled
+// body (64, 128, 256; the body fixes its own radices).  Grids it does not cover (another
+// time axis, nx not a multiple of the tile, the shipped Q2 launch grid) run the generic
+// tile body at the same CTA size with the fallback radix: the variant's radix in FP32,
+// radix 4 (the register form) in FP64.
 constexpr int kLineForm = 256;
 inline int line_pixels(bool fp64) { return fp64 ? 4 : 8; }  // pixels per tile
 inline bool is_line(PassVariant v) { return (v.r1 & kLineForm) != 0; }
 inline int radix_of(PassVariant v) { return v.r1 & (kLineForm - 1); }
-// Line-specialised t-pass kernels: CTA size and first-stage radix; (time axis, radix)
-// pairs with a compiled body.
-inline bool line_variant_compiled(int threads, int r1) { return threads == 128 && (r1 == 8 || r1 == 16); }
+// Line-specialised t-pass kernels: CTA size and the radix of the generic fallback.
+inline bool line_variant_compiled(int threads, int r1) { return threads == 128 && (r1 == 4 || r1 == 8 || r1 == 16); }
+inline int line_fallback_radix(bool fp64, PassVariant v) { return fp64 ? 4 : radix_of(v); }
+// First-stage radix of the compiled line body for a time axis of n samples (0: none).
+inline int line_radix(int n) { return (n == 256 || n == 128) ? 16 : (n == 64 ? 8 : 0); }
 // Largest radix of the generic fallback body at a line variant's CTA size.
 template <typename C, int THREADS> struct LineFallback {
     static constexpr int RMAX = (sizeof(C) == 16 && THREADS == 128) ? 8 : 16;
 };
-inline bool line_shape(int nt, int r1) { return (nt == 256 && r1 == 16) || (nt == 128 && r1 == 16) || (nt == 64 && r1 == 8); }
 
 inline bool is_ws(PassVariant v) { return v.threads == 160 || v.threads == 288; }
 inline int consumer_threads(PassVariant v) { return is_ws(v) ? v.threads - 32 : v.threads; }
@@ -204,9 +206,10 @@ inline bool variant_compiled(bool fp64, bool tpass, PassVariant v)
 template <typename C> cudaError_t launch_tpass(const TPassArgs<C> &a, PassVariant v, int grid, size_t smem,
                                                cudaStream_t st);
 // Line-specialised t-pass (v.r1 carries kLineForm) for a time axis of nt samples; nt = 0:
-// the generic tile body at the variant's CTA size and radix.
+// the generic tile body at the variant's CTA size with first-stage radix r_fallback
+// (the plan's).
 template <typename C>
-cudaError_t launch_tpass_line(const TPassArgs<C> &a, PassVariant v, int nt, int grid, size_t smem,
+cudaError_t launch_tpass_line(const TPassArgs<C> &a, PassVariant v, int nt, int r_fallback, int grid, size_t smem,
                               cudaStream_t st);
 // Dynamic shared memory of a line-specialised t-pass CTA (0: nt / r1 not compiled).
 size_t tpass_line_smem(bool fp64, int nt, int r1);

@@ -22,6 +22,9 @@ int solver_create_configured(const OpoParams *p, const double *w, const PassVari
                              cudaStream_t stream, OpoSolver **out);
 void solver_pass_info(const OpoSolver *s, int kind, int *ntiles, size_t *smem);
 PassVariant solver_pass_variant(const OpoSolver *s, int kind);
+// A line-specialised t-pass setting runs its line body on s's grid, or its generic
+// fallback with the setting's fallback radix (what a batch's kernel compiles).
+bool solver_line_fallback_ok(const OpoSolver *s);
 const OpoParams &solver_params(const OpoSolver *s);
 size_t solver_device_bytes(const OpoSolver *s);
 void *solver_field(OpoSolver *s, int which);

@@ -29,10 +29,10 @@ __global__ void __launch_bounds__(THREADS, 4) tpass_line_fallback_kernel(TPassAr
 }
 
 // Compiled line bodies: (time axis, first-stage radix), CTAs of 128 threads.  Fallback
-// radices: FP32 8 and 16, FP64 4.
+// radices: FP32 4, 8 and 16, FP64 4.
 #define OPO_LINE_SHAPES(X, C) X(C, 256, 16) X(C, 128, 16) X(C, 64, 8)
 #define OPO_LINE_ALL(X) OPO_LINE_SHAPES(X, float2) OPO_LINE_SHAPES(X, double2)
-#define OPO_LINE_FALLBACKS(X) X(float2, 16) X(float2, 8) X(double2, 4)
+#define OPO_LINE_FALLBACKS(X) X(float2, 16) X(float2, 8) X(float2, 4) X(double2, 4)
 
 size_t tpass_line_smem(bool fp64, int nt, int r1)
 {
@@ -62,9 +62,10 @@ cudaError_t configure_line_kernels(size_t smem)
 }
 
 template <typename C>
-cudaError_t launch_tpass_line(const TPassArgs<C> &a, PassVariant v, int nt, int grid, size_t smem, cudaStream_t st)
+cudaError_t launch_tpass_line(const TPassArgs<C> &a, PassVariant v, int nt, int r_fallback, int grid, size_t smem,
+                              cudaStream_t st)
 {
-    const int r1 = radix_of(v);
+    const int r1 = nt ? line_radix(nt) : r_fallback;
     const void *fn = nullptr;
 #define OPO_FN_L(CC, NT, RA)                                                                        \
     if constexpr (std::is_same<C, CC>::value)                                                       \
@@ -83,7 +84,9 @@ cudaError_t launch_tpass_line(const TPassArgs<C> &a, PassVariant v, int nt, int 
     return cudaLaunchKernel(fn, dim3(grid), dim3(v.threads), args, smem, st);
 }
 
-template cudaError_t launch_tpass_line<float2>(const TPassArgs<float2> &, PassVariant, int, int, size_t, cudaStream_t);
-template cudaError_t launch_tpass_line<double2>(const TPassArgs<double2> &, PassVariant, int, int, size_t, cudaStream_t);
+template cudaError_t launch_tpass_line<float2>(const TPassArgs<float2> &, PassVariant, int, int, int, size_t,
+                                              cudaStream_t);
+template cudaError_t launch_tpass_line<double2>(const TPassArgs<double2> &, PassVariant, int, int, int, size_t,
+                                               cudaStream_t);
 
 }  // namespace opo

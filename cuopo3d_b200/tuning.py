@@ -3,14 +3,26 @@
 A batch runs every instance with one kernel variant per pass (threads, tile elements,
 first-stage radix; opo_batch_create), so the best choice depends on the mix, not on
 any single grid.  The candidates are the single-instance autotuner's choices for each
-distinct grid of the mix (opo_autotune, cached per grid); each candidate that every
-instance of the mix accepts is timed on the whole mix for a few batched round trips,
-and the fastest is kept.  The reference has no batching and compile-time block sizes
+distinct grid of the mix (opo_autotune, cached per grid), and for a choice with the
+line-specialised t-pass also the same choice with the generic t-pass of its fallback
+radix (the batched kernels run the line body per instance, and a mix of time axes may
+prefer the generic one); each candidate that every instance of the mix accepts is timed
+on the whole mix for a few batched round trips, and the fastest is kept.  The reference has no batching and compile-time block sizes
 (DtypesConsts.cuh:48-50).
 """
 import time
 
-from . import Batch, OpoError, Simulation, derive, time_freq
+from . import FP64, LINE, Batch, OpoError, Simulation, derive, time_freq
+
+
+def generic_t(precision, tuning):
+    """`tuning` with its line-specialised t-pass replaced by the generic t-pass of the
+    line setting's fallback radix (FP32: its radix, FP64: 4)."""
+    t = dict(tuning["t"])
+    if not t["r1"] & LINE:
+        return tuning
+    t["r1"] = 4 if precision == FP64 else t["r1"] - LINE
+    return {**tuning, "t": t}
 
 
 def grid_tunings(precision, cfgs):
@@ -57,8 +69,9 @@ def tune_batch(precision, cfgs, hbm_budget, seeds=None, round_trips=2):
     seeds = seeds if seeds is not None else [1000 + k for k in range(len(cfgs))]
     cands = []
     for t in grid_tunings(precision, cfgs).values():
-        if t not in cands:
-            cands.append(t)
+        for c in (t, generic_t(precision, t)):
+            if c not in cands:
+                cands.append(c)
     timed = [(t, time_batch(precision, cfgs, t, hbm_budget, seeds, round_trips=round_trips)) for t in cands]
     ok = [(t, s) for t, s in timed if s is not None]
     if not ok:

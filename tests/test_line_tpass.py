@@ -1,10 +1,11 @@
-"""Line-specialised t-pass (tuning r1 + co.LINE): compile-time time axes 64, 128 and 256,
-tiles of 8 FP32 pixels (two per packed f32x2 instruction) or 4 FP64 pixels.  It must match
-the FP64 oracle within the form's tolerance (FP32 1e-5, FP64 1e-10; round trips with GDD,
-mirrors, EOM, the corrected physics with a phase mismatch, the closing pass's
-untransformed pump), agree with the generic kernel to rounding, fall back to the generic
-kernel on grids it does not cover, and give bit-identical results in a batch and in a
-standalone solver (the batched kernel runs the same tile body per instance)."""
+"""Line-specialised t-pass (tuning r1 + co.LINE): compiled bodies for the time axes 64,
+128 and 256, tiles of 8 FP32 pixels (two per packed f32x2 instruction) or 4 FP64 pixels.
+It must match the FP64 oracle within the form's tolerance (FP32 1e-5, FP64 1e-10; round
+trips with GDD, mirrors, EOM, the corrected physics with a phase mismatch, the closing
+pass's untransformed pump), agree with the generic kernel to rounding, fall back to the
+generic kernel with the setting's fallback radix (FP32: its r1, FP64: 4) on grids it does
+not cover, and give bit-identical results in a batch and in a standalone solver (the
+batched kernel runs the same tile bodies per instance)."""
 import numpy as np
 import pytest
 
@@ -80,15 +81,15 @@ def test_line_tpass_vs_oracle_and_generic(grid, r1, over, precision):
 @pytest.mark.parametrize("grid,over", [((16, 8, 96), {}), ((6, 8, 128), dict(flags=co.DISPERSION)),
                                        ((16, 16, 256), dict(flags=co.DISPERSION | co.DIFFRACTION | co.ASIS_Q2))])
 def test_line_tuning_falls_back_to_generic_kernel(grid, over, precision):
-    """Grids without a line body (time axis 96, nx = 6 not a multiple of the tile, the
-    shipped Q2 launch grid) keep the line setting but run the generic tile body (FP64: its radix-4
-    register form): bit for bit the generic kernel's results, and the oracle's within the
-    form's tolerance."""
+    """Grids without a line body (time axis 96, nx not a multiple of the tile, the shipped
+    Q2 launch grid) keep the line setting but run the generic tile body with the fallback
+    radix (FP32 the setting's 16, FP64 4 whatever the setting): bit for bit the generic
+    kernel's results, and the oracle's within the form's tolerance."""
     out, kw, flags, s0, t = run(grid, over, tuning(16, nt=grid[2]), precision)
-    assert t["r1"] & co.LINE
+    assert t["r1"] == 16 + co.LINE
     for a, b in zip(out, oracle(kw, flags, s0)):
         assert rel_l2(a, b) < TOL[precision]
-    gen, *_ = run(grid, over, tuning(t["r1"] - co.LINE, line=False, nt=grid[2]), precision)
+    gen, *_ = run(grid, over, tuning(4 if precision == co.FP64 else 16, line=False, nt=grid[2]), precision)
     for a, b in zip(out, gen):
         assert np.array_equal(a, b)
 
@@ -126,23 +127,19 @@ def test_line_tpass_full_size_vs_fp64():
 
 @pytest.mark.parametrize("precision", [co.FP32, co.FP64])
 def test_line_tpass_batch_equals_standalone(precision):
-    """A batch tuned to the line form, with instances on line axes (256, 128) and, in FP32,
-    one without (96: the generic body in the same launch; an FP64 instance without a line
-    body takes radix 4 and is refused): every slot bit for bit its standalone solver."""
+    """A batch tuned to the line form, with instances on every line axis (256, 128, 64) and
+    one without (96: the generic body with the fallback radix in the same launch): every
+    slot bit for bit its standalone solver."""
     base = dict(nz=4, LX=300.0, LY=300.0, Lcr=3000.0, FWHM=3.0, t_window=25.0, pump_mode="focused-pulsed",
                 total_rt=3, precision=precision)
     insts = [dict(nx=16, ny=16, nt=256, P=300.0, w0=40.0, gdd_gamma=1.0),
              dict(nx=32, ny=16, nt=128, P=150.0, w0=60.0, detuning=0.7, Rs=0.9),
              dict(nx=24, ny=24, nt=128, P=80.0, w0=50.0, flags=co.DISPERSION | co.DIFFRACTION | co.PHYSICS,
-                  Lambda=6.5)]
-    other = dict(nx=16, ny=16, nt=96, P=500.0, w0=35.0, detuning=-1.2)
+                  Lambda=6.5),
+             dict(nx=16, ny=32, nt=64, P=200.0, w0=45.0, detuning=0.3),
+             dict(nx=16, ny=16, nt=96, P=500.0, w0=35.0, detuning=-1.2)]
     tun = {"t": dict(threads=128, tile=2048, r1=16 + co.LINE), **AXES}
     b = co.Batch(precision, 8, 8 << 30, tuning=tun)
-    if precision == co.FP32:
-        insts.append(other)
-    else:
-        with pytest.raises(co.OpoError):
-            b.add(co.make_config(**{**base, **other}))
     slots = []
     for k, inst in enumerate(insts):
         cfg = co.make_config(**{**base, **inst})
