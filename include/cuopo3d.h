@@ -240,11 +240,11 @@ int opo_set_tuning(OpoSolver *s, const int tuning[9]);
  * kernels: 128 or 256 consumer threads plus one producer warp that streams the tiles
  * into a two-stage shared-memory ring with TMA (t- and y-passes in both precisions,
  * x-pass in FP64); batches run such a setting as its consumer CTA size.  A t-pass radix
- * with OPO_TUNE_LINE added (128 threads, radix 8 or 16) selects the line-specialised
- * t-pass: a compiled time axis (64 with radix 8; 128 or 256 with radix 16) and tiles of
- * 8 FP32 pixels (two per packed instruction) or 4 FP64 pixels; other grids (and the
- * shipped Q2 launch grid) run the generic kernel of the same size and radix (FP64:
- * radix 4).  No counterpart in the reference. */
+ * with OPO_TUNE_LINE added (128 threads) selects the line-specialised t-pass: compiled
+ * bodies for the time axes 64, 128 and 256, tiles of 8 FP32 pixels (two per packed
+ * instruction) or 4 FP64 pixels; other grids (and the shipped Q2 launch grid) run the
+ * generic kernel of the same size with the fallback radix (FP32: the given radix, FP64:
+ * 4).  No counterpart in the reference. */
 #define OPO_TUNE_LINE 256
 int opo_get_tuning(const OpoSolver *s, int out[9]);
 
