@@ -338,6 +338,8 @@ def run_ours(args):
         fp64_peak = co.fp64_peak()
         flops_t = V * 558.0
         ach_tf = flops_t / (t["avg_us"] * 1e-6) / 1e12 if t else None
+        t_kernel = ("tpass_line_kernel<double2, 256, 16, 128>" if main["tuning"]["t"]["r1"] & 256
+                    else "tpass_kernel<double2>")
         line = {
             "metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": main["ms_per_step"],
@@ -351,13 +353,13 @@ def run_ours(args):
             "e2e_pipelined": main["e2e_pipelined"],
             "gpu_launches": main["launches"],
             "clocks": main["clocks"],
-            "roofline": {"bound": "hbm", "kernel": "tpass_kernel<double2> (RK4 x2 + t-axis FFT pair)",
+            "roofline": {"bound": "hbm", "kernel": f"{t_kernel} (RK4 x2 + t-axis FFT pair)",
                          "achieved": achieved, "peak": hbm,
                          "peak_kind": f"{hbm_kind} (MEASURED_PEAKS.json hbm_gbs)" if hbm_kind == "measured" else "fallback",
                          "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
                          "traffic": ncu_traffic("tpass", "fp64"),
                          "alg_bytes_per_launch": V * 96},
-            "roofline_fp64_pipe": {"bound": "fp64", "kernel": "tpass_kernel<double2>", "achieved": ach_tf,
+            "roofline_fp64_pipe": {"bound": "fp64", "kernel": t_kernel, "achieved": ach_tf,
                                    "peak": fp64_peak, "peak_kind": "measured (opo_fp64_peak: FMA chains)",
                                    "unit": "TFLOP/s", "frac": (ach_tf / fp64_peak) if ach_tf else None,
                                    "alg_flops_per_launch": flops_t},
@@ -631,11 +633,11 @@ def run_reference(args):
 # Pinned kernel configurations of the bench workload (the autotuner's choices on a B200),
 # for profiling runs whose launch order must not depend on a timing-based choice.
 PINNED_TUNING = {
-    # t: the line-specialised FP32 t-pass (first-stage radix 16 + the line flag 256)
+    # t: the line-specialised t-pass (its fallback radix + the line flag 256)
     "fp32": {"t": dict(threads=128, tile=2048, r1=16 + 256), "x": dict(threads=128, tile=2048, r1=8),
              "y": dict(threads=128, tile=2048, r1=16)},
-    "fp64": {"t": dict(threads=128, tile=1024, r1=4), "x": dict(threads=160, tile=1024, r1=8),
-             "y": dict(threads=288, tile=2048, r1=8)},
+    "fp64": {"t": dict(threads=128, tile=1024, r1=4 + 256), "x": dict(threads=160, tile=1024, r1=8),
+             "y": dict(threads=160, tile=1024, r1=8)},
 }
 
 
