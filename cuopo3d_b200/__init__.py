@@ -91,6 +91,10 @@ def lib():
         L.opo_get_field.argtypes = [vp, _i, vp, _i, _i]
         L.opo_run_single_pass.argtypes = [vp]
         L.opo_run_round_trips.argtypes = [vp, _i]
+        L.opo_stream_put.argtypes = [vp, _i, vp, _i]
+        L.opo_stream_run.argtypes = [vp, _i]
+        L.opo_stream_get.argtypes = [vp, _i, vp, _i]
+        L.opo_stream_wait.argtypes = [vp]
         L.opo_field_sums.argtypes = [vp, dp]
         L.opo_synchronize.argtypes = [vp]
         L.opo_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
@@ -333,6 +337,21 @@ class Simulation:
 
     def synchronize(self):
         self._check(lib().opo_synchronize(self._h))
+
+    # Streamed round trips (opo_stream_*): `ptr` is the address of pinned host memory
+    # holding (put) or receiving (get) one field in the solver's precision; the calls
+    # return at once and the buffers stay in use until stream_wait().
+    def stream_put(self, which, ptr):
+        self._check(lib().opo_stream_put(self._h, which, ctypes.c_void_p(ptr), self.params.precision))
+
+    def stream_run(self, n=1):
+        self._check(lib().opo_stream_run(self._h, n))
+
+    def stream_get(self, which, ptr):
+        self._check(lib().opo_stream_get(self._h, which, ctypes.c_void_p(ptr), self.params.precision))
+
+    def stream_wait(self):
+        self._check(lib().opo_stream_wait(self._h))
 
     @property
     def round_trip_index(self):

@@ -339,6 +339,18 @@ struct OpoSolver {
     long long launches = 0;
     int launches_rt[2] = {0, 0};
     bool gdd_or_mirror = false;
+    // streamed round trips (opo_stream_*): device stages of the four fields for the uploads
+    // of the next run and the downloads of the last one, their copy streams and events
+    struct Streamed {
+        void *in[4] = {}, *out[4] = {};
+        unsigned staged = 0;         // fields uploaded into `in` since the last run
+        bool has_out = false;        // a run filled `out`
+        cudaStream_t cs_in = nullptr, cs_out = nullptr;
+        cudaEvent_t in_free = nullptr;   // compute stream: `in` copied into the fields
+        cudaEvent_t in_ready = nullptr;  // cs_in: the uploads so far landed
+        cudaEvent_t out_ready = nullptr; // compute stream: `out` holds the last run's fields
+        cudaEvent_t out_free = nullptr;  // cs_out: the downloads so far left `out`
+    } st;
     // per-pass event timing
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -1631,6 +1643,17 @@ void opo_destroy(OpoSolver *s)
         cudaEventDestroy(t.b);
     }
     for (auto e : s->ev_pool) cudaEventDestroy(e);
+    for (cudaStream_t c : {s->st.cs_in, s->st.cs_out})
+        if (c) {
+            cudaStreamSynchronize(c);
+            cudaStreamDestroy(c);
+        }
+    for (cudaEvent_t e : {s->st.in_free, s->st.in_ready, s->st.out_ready, s->st.out_free})
+        if (e) cudaEventDestroy(e);
+    for (int k = 0; k < 4; k++) {
+        if (s->st.in[k]) cudaFree(s->st.in[k]);
+        if (s->st.out[k]) cudaFree(s->st.out[k]);
+    }
     for (auto *f : s->field)
         if (f) cudaFree(f);
     if (s->partials) cudaFree(s->partials);
@@ -1735,6 +1758,94 @@ int opo_run_round_trips_tallied(OpoSolver *s, int n, double *tallies, int *done)
         if (rc) return rc;
     }
     return OPO_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Streamed round trips: uploads for the next run and downloads of the last run go through
+// device stages on two copy streams, so they overlap the round trips on the compute
+// stream.  Ordering (events): an upload waits until the previous run has taken `in`; a run
+// waits for the uploads, copies `in` into the fields, runs, waits until the previous
+// downloads left `out`, and copies the fields into `out`; a download waits for that run.
+
+static int stream_setup(OpoSolver *s)
+{
+    auto &st = s->st;
+    if (st.cs_in) return OPO_OK;
+    OPO_CU(s, cudaStreamCreateWithFlags(&st.cs_in, cudaStreamNonBlocking), "stream create");
+    OPO_CU(s, cudaStreamCreateWithFlags(&st.cs_out, cudaStreamNonBlocking), "stream create");
+    for (cudaEvent_t *e : {&st.in_free, &st.in_ready, &st.out_ready, &st.out_free})
+        OPO_CU(s, cudaEventCreateWithFlags(e, cudaEventDisableTiming), "event create");
+    return OPO_OK;
+}
+
+int opo_stream_put(OpoSolver *s, int which, const void *host, int prec)
+{
+    if (!s) return OPO_ERR_INVALID;
+    if (which < 0 || which > 3 || !host || prec != s->p.precision)
+        return fail(s, OPO_ERR_INVALID, "opo_stream_put: bad argument (host data in the solver's precision)");
+    if (int rc = stream_setup(s)) return rc;
+    auto &st = s->st;
+    const size_t bytes = s->esz * s->V;
+    if (!st.in[which]) OPO_CU(s, cudaMalloc(&st.in[which], bytes), "cudaMalloc(stream stage)");
+    OPO_CU(s, cudaStreamWaitEvent(st.cs_in, st.in_free, 0), "stream wait");
+    OPO_CU(s, cudaMemcpyAsync(st.in[which], host, bytes, cudaMemcpyHostToDevice, st.cs_in), "stream upload");
+    OPO_CU(s, cudaEventRecord(st.in_ready, st.cs_in), "event record");
+    st.staged |= 1u << which;
+    return OPO_OK;
+}
+
+int opo_stream_run(OpoSolver *s, int n)
+{
+    if (!s || n < 0) return s ? fail(s, OPO_ERR_INVALID, "negative round-trip count") : OPO_ERR_INVALID;
+    if (int rc = stream_setup(s)) return rc;
+    auto &st = s->st;
+    const size_t bytes = s->esz * s->V;
+    if (st.staged) {
+        OPO_CU(s, cudaStreamWaitEvent(s->stream, st.in_ready, 0), "stream wait");
+        for (int k = 0; k < 4; k++)
+            if (st.staged & (1u << k)) {
+                OPO_CU(s, cudaMemcpyAsync(s->field[k], st.in[k], bytes, cudaMemcpyDeviceToDevice, s->stream),
+                       "stream stage copy");
+                s->reloaded |= 1u << k;
+            }
+        OPO_CU(s, cudaEventRecord(st.in_free, s->stream), "event record");
+        if (s->reloaded == 0xfu) s->fields_lost = false;
+        st.staged = 0;
+    }
+    if (int rc = opo_run_round_trips(s, n)) return rc;
+    OPO_CU(s, cudaStreamWaitEvent(s->stream, st.out_free, 0), "stream wait");
+    for (int k = 0; k < 4; k++) {
+        if (!st.out[k]) OPO_CU(s, cudaMalloc(&st.out[k], bytes), "cudaMalloc(stream stage)");
+        OPO_CU(s, cudaMemcpyAsync(st.out[k], s->field[k], bytes, cudaMemcpyDeviceToDevice, s->stream),
+               "stream stage copy");
+    }
+    OPO_CU(s, cudaEventRecord(st.out_ready, s->stream), "event record");
+    st.has_out = true;
+    return OPO_OK;
+}
+
+int opo_stream_get(OpoSolver *s, int which, void *host, int prec)
+{
+    if (!s) return OPO_ERR_INVALID;
+    if (which < 0 || which > 3 || !host || prec != s->p.precision)
+        return fail(s, OPO_ERR_INVALID, "opo_stream_get: bad argument (host data in the solver's precision)");
+    auto &st = s->st;
+    if (!st.has_out) return fail(s, OPO_ERR_INVALID, "opo_stream_get before any opo_stream_run");
+    OPO_CU(s, cudaStreamWaitEvent(st.cs_out, st.out_ready, 0), "stream wait");
+    OPO_CU(s, cudaMemcpyAsync(host, st.out[which], s->esz * s->V, cudaMemcpyDeviceToHost, st.cs_out),
+           "stream download");
+    OPO_CU(s, cudaEventRecord(st.out_free, st.cs_out), "event record");
+    return OPO_OK;
+}
+
+int opo_stream_wait(OpoSolver *s)
+{
+    if (!s) return OPO_ERR_INVALID;
+    auto &st = s->st;
+    if (st.cs_in) OPO_CU(s, cudaStreamSynchronize(st.cs_in), "stream sync");
+    OPO_CU(s, cudaStreamSynchronize(s->stream), "stream sync");
+    if (st.cs_out) OPO_CU(s, cudaStreamSynchronize(st.cs_out), "stream sync");
+    return check_pass_error(s);
 }
 
 int opo_set_wait_limit(OpoSolver *s, long long cycles)

@@ -197,6 +197,26 @@ int opo_run_single_pass(OpoSolver *s);
  * (skipped on round trip total_rt-1), GDD compensation, mirrors. */
 int opo_run_round_trips(OpoSolver *s, int n);
 
+/* Streamed round trips, for a host that feeds a solver one step after another (a sweep
+ * point per step): the copies of the next step's inputs and of the last step's results
+ * run on two copy streams while the round trips run, through device stages of the four
+ * fields (allocated at first use: 8 x the field size).  All four calls return without
+ * waiting; host buffers must be pinned and in the solver's precision, and must stay
+ * untouched until opo_stream_wait.
+ *   opo_stream_put  enqueue the upload of field `which` for the next opo_stream_run
+ *                   (it lands in the field when that run starts);
+ *   opo_stream_run  the uploaded fields go into place, n round trips run
+ *                   (opo_run_round_trips), and the four fields are kept for download;
+ *   opo_stream_get  enqueue the download of field `which` as the last opo_stream_run
+ *                   left it (later runs do not overwrite it before it is copied);
+ *   opo_stream_wait block until every streamed copy and round trip has completed.
+ * No counterpart in the reference, whose main runs one configuration per process and
+ * reads every saved field back with a blocking copy (cuOPO3D.cu:75-85). */
+int opo_stream_put(OpoSolver *s, int which, const void *host, int elem_precision);
+int opo_stream_run(OpoSolver *s, int n);
+int opo_stream_get(OpoSolver *s, int which, void *host, int elem_precision);
+int opo_stream_wait(OpoSolver *s);
+
 /* FP64 sum of |A|^2 over every voxel of the pump, signal and idler (in that order);
  * the reference's averagePowerCutXY (Solver3D.cuh:529-545) is
  * 0.5 eps0 c ns dx dy / (LX LY) times the signal entry. */
