@@ -34,14 +34,15 @@ __global__ void __launch_bounds__(THREADS, 4) tpass_line_fallback_kernel(TPassAr
 #define OPO_LINE_ALL(X) OPO_LINE_SHAPES(X, float2) OPO_LINE_SHAPES(X, double2)
 #define OPO_LINE_FALLBACKS(X) X(float2, 16) X(float2, 8) X(float2, 4) X(double2, 4)
 
-size_t tpass_line_smem(bool fp64, int nt, int r1)
+// A tile and its twiddles (the units are 16 bytes in both precisions; the twiddles are C).
+template <typename C> size_t line_smem(int nt, int r1)
 {
-    (void)fp64;  // a unit is 16 bytes in both precisions
-    if (nt == 256 && r1 == 16) return LineGeom<float2, 256, 16>::tile_bytes();
-    if (nt == 128 && r1 == 16) return LineGeom<float2, 128, 16>::tile_bytes();
-    if (nt == 64 && r1 == 8) return LineGeom<float2, 64, 8>::tile_bytes();
+    if (nt == 256 && r1 == 16) return LineGeom<C, 256, 16>::tile_bytes();
+    if (nt == 128 && r1 == 16) return LineGeom<C, 128, 16>::tile_bytes();
+    if (nt == 64 && r1 == 8) return LineGeom<C, 64, 8>::tile_bytes();
     return 0;
 }
+size_t tpass_line_smem(bool fp64, int nt, int r1) { return fp64 ? line_smem<double2>(nt, r1) : line_smem<float2>(nt, r1); }
 
 cudaError_t configure_line_kernels(size_t smem)
 {

@@ -19,7 +19,9 @@
 // Shared memory per field: NT + NT / RB rows of four units; time sample t sits in row
 // t + t / RB (a padding row after every RB rows), so the RB-point stage's eight
 // butterflies of a warp fall on alternating halves of the banks, and the other stages
-// read whole 512-byte runs.
+// read whole 512-byte runs.  The first stage's twiddles are staged with the tile, after
+// the three field regions (shared-memory latency instead of L1 for the 30 twiddle loads
+// of a first- and last-stage item; the phase tables stay in global memory).
 //
 // The single-instance kernel runs one tile per CTA, four CTAs of 128 threads per SM; the
 // batched kernel runs the same body over the tiles of every instance.
@@ -252,8 +254,9 @@ template <typename C, int NT, int RA> struct LineGeom {
     __device__ __forceinline__ static constexpr int row(int t) { return t + t / RB; }
     // byte offset of (field f, time sample t, unit u) in a tile buffer
     __device__ __forceinline__ static constexpr int at(int f, int t, int u) { return f * REGION + (row(t) * PP + u) * 16; }
+    static constexpr int NTW = (RA - 1) * Q;  // first-stage twiddles, staged after the tile
     static constexpr int TILE_BYTES = 3 * REGION;
-    static constexpr size_t tile_bytes() { return (size_t)TILE_BYTES; }
+    static constexpr size_t tile_bytes() { return (size_t)TILE_BYTES + (size_t)NTW * sizeof(C); }
 };
 
 // Issue the cp.async copies of tile `tile` (the fields in lmask) into buffer buf.
@@ -332,7 +335,9 @@ __device__ __forceinline__ void line_stage_a(const TPassArgs<C> &a, unsigned cha
     for (int m = 0; m < RA; m++) x[m] = L::lds(buf + G::at(f, j + Q * m, u));
     L::template dft<RA, +1>(x);
 #pragma unroll
-    for (int k = 1; k < RA; k++) x[k] = L::template tmul<true>(x[k], __ldg(a.tw + (k - 1) * Q + j));
+    const C *tws = reinterpret_cast<const C *>(buf + G::TILE_BYTES);
+#pragma unroll
+    for (int k = 1; k < RA; k++) x[k] = L::template tmul<true>(x[k], tws[(k - 1) * Q + j]);
 #pragma unroll
     for (int k = 0; k < RA; k++) L::sts(buf + G::at(f, j + Q * k, u), x[k]);
 }
@@ -382,7 +387,9 @@ __device__ __forceinline__ void line_stage_c(const TPassArgs<C> &a, const unsign
 #pragma unroll
     for (int m = 0; m < RA; m++) x[m] = L::lds(buf + G::at(f, j + Q * m, u));
 #pragma unroll
-    for (int m = 1; m < RA; m++) x[m] = L::template tmul<false>(x[m], __ldg(a.tw + (m - 1) * Q + j));
+    const C *tws = reinterpret_cast<const C *>(buf + G::TILE_BYTES);
+#pragma unroll
+    for (int m = 1; m < RA; m++) x[m] = L::template tmul<false>(x[m], tws[(m - 1) * Q + j]);
     L::template dft<RA, -1>(x);
     C *d = a.f[f] + base + (unsigned)j * gs + u * L::PX;
 #pragma unroll
@@ -440,6 +447,11 @@ __device__ __forceinline__ void tpass_line_tile(const TPassArgs<C> &a, unsigned 
     const unsigned base = tile_base(a.g, tile);
     const unsigned tmask = a.tmask, lmask = tpass_load_mask(a);
     line_stage_in<C, NT, RA, THREADS>(a, tile, lmask, buf);
+    {  // the first stage's twiddles
+        using G = LineGeom<C, NT, RA>;
+        C *tws = reinterpret_cast<C *>(buf + G::TILE_BYTES);
+        for (int e = threadIdx.x; e < G::NTW; e += THREADS) cp_async<sizeof(C)>(tws + e, a.tw + e);
+    }
     cp_async_wait_all();
     tile_sync<BAR>();
     line_sweep<C, NT, RA, THREADS>(a, base, lmask, tmask, buf);
