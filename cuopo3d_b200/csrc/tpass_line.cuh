@@ -334,7 +334,6 @@ __device__ __forceinline__ void line_stage_a(const TPassArgs<C> &a, unsigned cha
 #pragma unroll
     for (int m = 0; m < RA; m++) x[m] = L::lds(buf + G::at(f, j + Q * m, u));
     L::template dft<RA, +1>(x);
-#pragma unroll
     const C *tws = reinterpret_cast<const C *>(buf + G::TILE_BYTES);
 #pragma unroll
     for (int k = 1; k < RA; k++) x[k] = L::template tmul<true>(x[k], tws[(k - 1) * Q + j]);
@@ -386,7 +385,6 @@ __device__ __forceinline__ void line_stage_c(const TPassArgs<C> &a, const unsign
     typename L::U x[RA];
 #pragma unroll
     for (int m = 0; m < RA; m++) x[m] = L::lds(buf + G::at(f, j + Q * m, u));
-#pragma unroll
     const C *tws = reinterpret_cast<const C *>(buf + G::TILE_BYTES);
 #pragma unroll
     for (int m = 1; m < RA; m++) x[m] = L::template tmul<false>(x[m], tws[(m - 1) * Q + j]);
