@@ -26,9 +26,13 @@
 
 namespace opo {
 
+// One launch's share of a descriptor array: instances [first, first + ninst) with their
+// tile prefix at prefix[pfirst ...] (starting at 0), total_tiles tiles.
 struct BatchHeader {
     unsigned ninst;
     unsigned total_tiles;
+    unsigned first;
+    unsigned pfirst;
 };
 
 template <typename Args> __host__ __device__ constexpr unsigned desc_bytes() { return (unsigned)((sizeof(Args) + 127) / 128 * 128); }
@@ -60,6 +64,8 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 4 : 1)
     TPassArgs<C> *d = reinterpret_cast<TPassArgs<C> *>(smem_raw);
     C *sm = reinterpret_cast<C *>(smem_raw + desc_bytes<TPassArgs<C>>());
     const unsigned ninst = hdr->ninst, total = hdr->total_tiles;
+    descs += hdr->first;
+    prefix += hdr->pfirst;
     int cur = -1;
     for (unsigned gt = blockIdx.x; gt < total; gt += gridDim.x) {
         const int i = find_inst(prefix, ninst, gt);
@@ -79,17 +85,20 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 4 : 1)
     }
 }
 
-// Batched line-specialised t-pass: instances whose grid has a line body (line_nt: 256,
-// 128, 64) run it (one tile at a time, one tile buffer), the others the generic body of
-// the same CTA size with the setting's fallback radix RF.
-template <typename C, int RF, int THREADS>
-__global__ void __launch_bounds__(THREADS, 3)
+// Batched line-specialised t-pass for the instances whose time axis has the line body
+// (NT, RA): one tile at a time, one tile buffer.  Each line body has a kernel of its own
+// (one kernel holding every body and the generic one needed 168 registers and spilled);
+// the instances without a line body run tpass_batch_kernel with the fallback radix.
+template <typename C, int NT, int RA, int THREADS>
+__global__ void __launch_bounds__(THREADS, 4)
     tpass_line_batch_kernel(const TPassArgs<C> *descs, const unsigned *prefix, const BatchHeader *hdr, int tp)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TPassArgs<C> *d = reinterpret_cast<TPassArgs<C> *>(smem_raw);
     unsigned char *buf = smem_raw + desc_bytes<TPassArgs<C>>();
     const unsigned ninst = hdr->ninst, total = hdr->total_tiles;
+    descs += hdr->first;
+    prefix += hdr->pfirst;
     int cur = -1;
     for (unsigned gt = blockIdx.x; gt < total; gt += gridDim.x) {
         const int i = find_inst(prefix, ninst, gt);
@@ -101,19 +110,7 @@ __global__ void __launch_bounds__(THREADS, 3)
             __syncthreads();
             cur = i;
         }
-        const unsigned tile = gt - __ldg(prefix + i);
-        if (d->line_nt == 256) {
-            tpass_line_tile<C, 256, 16, THREADS>(*d, tile, buf);
-        } else if (d->line_nt == 128) {
-            tpass_line_tile<C, 128, 16, THREADS>(*d, tile, buf);
-        } else if (d->line_nt == 64) {
-            tpass_line_tile<C, 64, 8, THREADS>(*d, tile, buf);
-        } else {
-            C *sm = reinterpret_cast<C *>(buf);
-            const C *src[3] = {d->psrc, d->f[1], d->f[2]};
-            stage_tile<C, THREADS, false>(d->g, (unsigned)d->plan.n, tile, src, tpass_load_mask(*d), sm);
-            tpass_tile<C, RF, THREADS, LineFallback<C, THREADS>::RMAX, true>(*d, tile, sm);
-        }
+        tpass_line_tile<C, NT, RA, THREADS>(*d, gt - __ldg(prefix + i), buf);
     }
 }
 
@@ -125,6 +122,8 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 4 : 1)
     AxisArgs<C> *d = reinterpret_cast<AxisArgs<C> *>(smem_raw);
     C *sm = reinterpret_cast<C *>(smem_raw + desc_bytes<AxisArgs<C>>());
     const unsigned ninst = hdr->ninst, total = hdr->total_tiles;
+    descs += hdr->first;
+    prefix += hdr->pfirst;
     int cur = -1;
     for (unsigned gt = blockIdx.x; gt < total; gt += gridDim.x) {
         const int i = find_inst(prefix, ninst, gt);
@@ -200,21 +199,34 @@ __global__ void batch_tally_final_kernel(const double *partials, int nslots, dou
     X(float2, 256, 8, 16) X(float2, 256, 16, 16) X(double2, 128, 4, 8) X(double2, 128, 8, 8)        \
     X(double2, 256, 4, 16) X(double2, 256, 8, 16) X(double2, 256, 16, 16)
 
-// Resolves the batched kernel of a variant; returns false if it is not compiled.
-template <typename C> bool batch_t_func(PassVariant v, const void **fn)
+// t-pass groups: under the line-specialised setting, the instances with the 256-, 128-
+// and 64-sample line bodies (groups 0-2) and the rest (group 3, the generic body with the
+// fallback radix); under any other setting every instance is in group 3.
+constexpr int kTGroups = 4;
+inline int t_group(PassVariant v, int line_nt)
 {
-    if (is_line(v)) {
-        if (!line_variant_compiled(v.threads, radix_of(v))) return false;
-        if constexpr (sizeof(C) == 16) {
-            *fn = reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 4, 128>);
-        } else {
-            const int rf = line_fallback_radix(false, v);
-            *fn = rf == 16  ? reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 16, 128>)
-                  : rf == 8 ? reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 8, 128>)
-                            : reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 4, 128>);
-        }
-        return true;
-    }
+    if (!is_line(v)) return 3;
+    return line_nt == 256 ? 0 : line_nt == 128 ? 1 : line_nt == 64 ? 2 : 3;
+}
+constexpr int kLineGroupNT[3] = {256, 128, 64};
+
+template <typename C> bool batch_t_generic_func(PassVariant v, const void **fn);
+
+// Resolves the batched kernel of each t-pass group (nullptr: the group is never
+// populated under this setting); returns false if a variant is not compiled.
+template <typename C> bool batch_t_funcs(PassVariant v, const void *fn[kTGroups])
+{
+    for (int g = 0; g < kTGroups; g++) fn[g] = nullptr;
+    if (!is_line(v)) return batch_t_generic_func<C>(v, &fn[3]);
+    if (v.threads != 128 || !line_variant_compiled(v.threads, radix_of(v))) return false;
+    fn[0] = reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 256, 16, 128>);
+    fn[1] = reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 128, 16, 128>);
+    fn[2] = reinterpret_cast<const void *>(tpass_line_batch_kernel<C, 64, 8, 128>);
+    return batch_t_generic_func<C>(PassVariant{128, line_fallback_radix(sizeof(C) == 16, v)}, &fn[3]);
+}
+
+template <typename C> bool batch_t_generic_func(PassVariant v, const void **fn)
+{
     bool ok = false;
 #define OPO_F_T(CC, T, R, RM)                                                                       \
     if constexpr (std::is_same<C, CC>::value) {                                                     \
@@ -280,16 +292,18 @@ struct OpoBatch {
     // device state
     void *d_t[3] = {};       // t descriptors: first, middle, final
     void *d_ax[2][2] = {};   // [x, y][crystal, free]
-    unsigned *d_prefix[3] = {};
-    opo::BatchHeader *d_hdr = nullptr;  // [3]
+    unsigned *d_prefix[3] = {};  // t: one prefix per t-pass group, back to back
+    opo::BatchHeader *d_hdr = nullptr;  // [t-pass groups..., x, y]
     opo::SlotFields *d_slotf = nullptr;
     double *d_partials = nullptr, *d_sums = nullptr;
     std::vector<unsigned char> h_desc;  // host staging
     bool dirty = true;
     std::vector<char> last_flag;  // per order position: on its last round trip when uploaded
     cudaGraphExec_t graph = nullptr;
-    size_t graph_smem[3] = {0, 0, 0};
+    size_t graph_smem[3] = {0, 0, 0};  // t: the generic group's
     int grid[3] = {0, 0, 0};
+    int t_grid[opo::kTGroups] = {};
+    size_t t_smem[opo::kTGroups] = {};
     long long launches = 0;
     int launches_rt = 0;
     std::string err;
@@ -325,7 +339,8 @@ template <typename C> int upload_descriptors(OpoBatch *b)
     std::vector<AA> ax[2][2];
     std::vector<unsigned> prefix[3];
     std::vector<opo::SlotFields> sf;
-    for (int k = 0; k < 3; k++) prefix[k].push_back(0);
+    std::vector<int> tgroup;
+    for (int k = 1; k < 3; k++) prefix[k].push_back(0);
     b->last_flag.assign(n, 0);
     for (int pos = 0; pos < n; pos++) {
         Slot &sl = b->slots[b->order[pos]];
@@ -347,7 +362,8 @@ template <typename C> int upload_descriptors(OpoBatch *b)
             ax[a][0].push_back(opo::make_axis_args<C>(s, 1 + a, 0, diff ? 7u : 0u));
             ax[a][1].push_back(opo::make_axis_args<C>(s, 1 + a, 1, (diff && !last) ? 6u : 0u));
         }
-        for (int k = 0; k < 3; k++) {
+        tgroup.push_back(opo::t_group(b->v[0], opo::solver_line_nt(s)));
+        for (int k = 1; k < 3; k++) {
             int nt;
             size_t sm;
             opo::solver_pass_info(s, k, &nt, &sm);
@@ -358,18 +374,37 @@ template <typename C> int upload_descriptors(OpoBatch *b)
         f.n = (unsigned long long)sl.voxels;
         sf.push_back(f);
     }
+    // t descriptors group-major, each group with its own tile prefix (from 0)
+    opo::BatchHeader hdr[opo::kTGroups + 2];
+    {
+        std::vector<TA> ts[3];
+        for (int g = 0; g < opo::kTGroups; g++) {
+            hdr[g].first = (unsigned)ts[0].size();
+            hdr[g].pfirst = (unsigned)prefix[0].size();
+            prefix[0].push_back(0);
+            for (int pos = 0; pos < n; pos++) {
+                if (tgroup[pos] != g) continue;
+                for (int k = 0; k < 3; k++) ts[k].push_back(t[k][pos]);
+                int nt;
+                size_t sm;
+                opo::solver_pass_info(b->slots[b->order[pos]].s, 0, &nt, &sm);
+                prefix[0].push_back(prefix[0].back() + (unsigned)nt);
+            }
+            hdr[g].ninst = (unsigned)ts[0].size() - hdr[g].first;
+            hdr[g].total_tiles = prefix[0].back();
+        }
+        for (int k = 0; k < 3; k++) t[k].swap(ts[k]);
+    }
     const size_t cap = (size_t)b->capacity;
     for (int k = 0; k < 3; k++)
         if (n) OPO_BCU(b, cudaMemcpyAsync(b->d_t[k], t[k].data(), sizeof(TA) * n, cudaMemcpyHostToDevice, b->stream), "descriptors");
     for (int a = 0; a < 2; a++)
         for (int w = 0; w < 2; w++)
             if (n) OPO_BCU(b, cudaMemcpyAsync(b->d_ax[a][w], ax[a][w].data(), sizeof(AA) * n, cudaMemcpyHostToDevice, b->stream), "descriptors");
-    opo::BatchHeader hdr[3];
-    for (int k = 0; k < 3; k++) {
-        OPO_BCU(b, cudaMemcpyAsync(b->d_prefix[k], prefix[k].data(), sizeof(unsigned) * (n + 1), cudaMemcpyHostToDevice, b->stream), "prefix");
-        hdr[k].ninst = (unsigned)n;
-        hdr[k].total_tiles = prefix[k].back();
-    }
+    for (int k = 0; k < 3; k++)
+        OPO_BCU(b, cudaMemcpyAsync(b->d_prefix[k], prefix[k].data(), sizeof(unsigned) * prefix[k].size(),
+                                   cudaMemcpyHostToDevice, b->stream), "prefix");
+    for (int a = 0; a < 2; a++) hdr[opo::kTGroups + a] = opo::BatchHeader{(unsigned)n, prefix[1 + a].back(), 0, 0};
     OPO_BCU(b, cudaMemcpyAsync(b->d_hdr, hdr, sizeof(hdr), cudaMemcpyHostToDevice, b->stream), "header");
     if (n) OPO_BCU(b, cudaMemcpyAsync(b->d_slotf, sf.data(), sizeof(opo::SlotFields) * n, cudaMemcpyHostToDevice, b->stream), "slot fields");
     // pageable sources: make the copies complete before the host vectors go away
@@ -391,25 +426,33 @@ template <typename C> int enqueue_batch_round_trip(OpoBatch *b)
 {
     using TA = opo::TPassArgs<C>;
     using AA = opo::AxisArgs<C>;
-    const void *ft = nullptr, *fx = nullptr, *fy = nullptr;
-    if (!opo::batch_t_func<C>(b->v[0], &ft) || !opo::batch_a_func<C>(b->v[1], true, &fx) ||
+    const void *ft[opo::kTGroups], *fx = nullptr, *fy = nullptr;
+    if (!opo::batch_t_funcs<C>(b->v[0], ft) || !opo::batch_a_func<C>(b->v[1], true, &fx) ||
         !opo::batch_a_func<C>(b->v[2], false, &fy))
         return bfail(b, OPO_ERR_INVALID, "batch kernel variant not compiled");
-    const size_t st = opo::desc_bytes<TA>() + b->graph_smem[0];
     const size_t sx = opo::desc_bytes<AA>() + b->graph_smem[1];
     const size_t sy = opo::desc_bytes<AA>() + b->graph_smem[2];
     const opo::BatchHeader *hdr = b->d_hdr;
+    // one launch per t-pass group the setting populates; a group without instances
+    // (its header counts none) returns at once
     auto launch_t = [&](int which, int tp) -> cudaError_t {
         const TA *descs = static_cast<const TA *>(b->d_t[which]);
         const unsigned *pre = b->d_prefix[0];
-        void *args[] = {(void *)&descs, (void *)&pre, (void *)&hdr, (void *)&tp};
-        b->launches++;
-        return cudaLaunchKernel(ft, dim3(b->grid[0]), dim3(b->v[0].threads), args, st, b->stream);
+        for (int g = 0; g < opo::kTGroups; g++) {
+            if (!ft[g]) continue;
+            const opo::BatchHeader *h = hdr + g;
+            void *args[] = {(void *)&descs, (void *)&pre, (void *)&h, (void *)&tp};
+            b->launches++;
+            cudaError_t e = cudaLaunchKernel(ft[g], dim3(b->t_grid[g]), dim3(b->v[0].threads), args, b->t_smem[g],
+                                             b->stream);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
     };
     auto launch_a = [&](int axis, int which) -> cudaError_t {
         const AA *descs = static_cast<const AA *>(b->d_ax[axis][which]);
         const unsigned *pre = b->d_prefix[1 + axis];
-        const opo::BatchHeader *h = hdr + 1 + axis;
+        const opo::BatchHeader *h = hdr + opo::kTGroups + axis;
         void *args[] = {(void *)&descs, (void *)&pre, (void *)&h};
         b->launches++;
         return cudaLaunchKernel(axis == 0 ? fx : fy, dim3(b->grid[1 + axis]), dim3(b->v[1 + axis].threads), args,
@@ -434,24 +477,35 @@ template <typename C> int build_batch_graph(OpoBatch *b)
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
     }
-    // shared memory: the largest tile of any slot, per pass kind
+    // shared memory: the largest tile of any slot, per pass kind (t: of the slots in the
+    // generic group; a line body's tile has a fixed size)
     for (int k = 0; k < 3; k++) b->graph_smem[k] = 0;
     for (int sidx : b->order) {
         for (int k = 0; k < 3; k++) {
             int nt;
             size_t sm;
             opo::solver_pass_info(b->slots[sidx].s, k, &nt, &sm);
+            if (k == 0 && opo::t_group(b->v[0], opo::solver_line_nt(b->slots[sidx].s)) != 3) continue;
             b->graph_smem[k] = std::max(b->graph_smem[k], sm);
         }
     }
-    const void *ft = nullptr, *fx = nullptr, *fy = nullptr;
-    if (!opo::batch_t_func<C>(b->v[0], &ft) || !opo::batch_a_func<C>(b->v[1], true, &fx) ||
+    const void *ft[opo::kTGroups], *fx = nullptr, *fy = nullptr;
+    if (!opo::batch_t_funcs<C>(b->v[0], ft) || !opo::batch_a_func<C>(b->v[1], true, &fx) ||
         !opo::batch_a_func<C>(b->v[2], false, &fy))
         return bfail(b, OPO_ERR_INVALID, "batch kernel variant not compiled");
-    const size_t sm[3] = {opo::desc_bytes<TA>() + b->graph_smem[0], opo::desc_bytes<AA>() + b->graph_smem[1],
-                          opo::desc_bytes<AA>() + b->graph_smem[2]};
-    const void *fns[3] = {ft, fx, fy};
-    for (int k = 0; k < 3; k++) {
+    const bool fp64 = sizeof(C) == 16;
+    for (int g = 0; g < opo::kTGroups; g++) {
+        if (!ft[g]) continue;
+        b->t_smem[g] = opo::desc_bytes<TA>() +
+                       (g < 3 ? opo::tpass_line_smem(fp64, opo::kLineGroupNT[g], opo::line_radix(opo::kLineGroupNT[g]))
+                              : b->graph_smem[0]);
+        if (b->t_smem[g] > 227 * 1024) return bfail(b, OPO_ERR_INVALID, "batched tile does not fit in shared memory");
+        OPO_BCU(b, cudaFuncSetAttribute(ft[g], cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "attribute");
+        b->t_grid[g] = persistent_grid(b, ft[g], b->v[0].threads, b->t_smem[g]);
+    }
+    const size_t sm[3] = {0, opo::desc_bytes<AA>() + b->graph_smem[1], opo::desc_bytes<AA>() + b->graph_smem[2]};
+    const void *fns[3] = {nullptr, fx, fy};
+    for (int k = 1; k < 3; k++) {
         if (sm[k] > 227 * 1024) return bfail(b, OPO_ERR_INVALID, "batched tile does not fit in shared memory");
         OPO_BCU(b, cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "attribute");
         b->grid[k] = persistent_grid(b, fns[k], b->v[k].threads, sm[k]);
@@ -493,6 +547,7 @@ template <typename C> int batch_run(OpoBatch *b, int n)
                 int nt;
                 size_t sm;
                 opo::solver_pass_info(b->slots[sidx].s, k, &nt, &sm);
+                if (k == 0 && opo::t_group(b->v[0], opo::solver_line_nt(b->slots[sidx].s)) != 3) continue;
                 if (sm > b->graph_smem[k]) rebuild = true;
             }
         if (rebuild) {
@@ -576,9 +631,10 @@ int opo_batch_create(int precision, int capacity, size_t hbm_budget, const int t
             for (int w = 0; w < 2 && !rc; w++)
                 if (cudaMalloc(&b->d_ax[a][w], asz * capacity) != cudaSuccess) rc = OPO_ERR_NOMEM;
         for (int k = 0; k < 3 && !rc; k++)
-            if (cudaMalloc((void **)&b->d_prefix[k], sizeof(unsigned) * (capacity + 1)) != cudaSuccess) rc = OPO_ERR_NOMEM;
+            if (cudaMalloc((void **)&b->d_prefix[k], sizeof(unsigned) * (capacity + opo::kTGroups)) != cudaSuccess)
+                rc = OPO_ERR_NOMEM;
         if (rc) break;
-        if (cudaMalloc((void **)&b->d_hdr, sizeof(opo::BatchHeader) * 3) != cudaSuccess ||
+        if (cudaMalloc((void **)&b->d_hdr, sizeof(opo::BatchHeader) * (opo::kTGroups + 2)) != cudaSuccess ||
             cudaMalloc((void **)&b->d_slotf, sizeof(opo::SlotFields) * capacity) != cudaSuccess ||
             cudaMalloc((void **)&b->d_partials, sizeof(double) * 3 * opo::kTallyBlocks * capacity) != cudaSuccess ||
             cudaMalloc((void **)&b->d_sums, sizeof(double) * 3 * capacity) != cudaSuccess) {

@@ -1983,6 +1983,8 @@ bool solver_line_fallback_ok(const OpoSolver *s)
     return pc.plan.radix[0] == line_fallback_radix(s->p.precision == OPO_FP64, pc.v);
 }
 
+int solver_line_nt(const OpoSolver *s) { return s->pass[kT].line_nt; }
+
 void solver_pass_info(const OpoSolver *s, int kind, int *ntiles, size_t *smem)
 {
     *ntiles = s->pass[kind].geo.ntiles;

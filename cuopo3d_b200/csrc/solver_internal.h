@@ -25,6 +25,8 @@ PassVariant solver_pass_variant(const OpoSolver *s, int kind);
 // A line-specialised t-pass setting runs its line body on s's grid, or its generic
 // fallback with the setting's fallback radix (what a batch's kernel compiles).
 bool solver_line_fallback_ok(const OpoSolver *s);
+// The line body's time axis the t-pass runs on s's grid (0: the generic body).
+int solver_line_nt(const OpoSolver *s);
 const OpoParams &solver_params(const OpoSolver *s);
 size_t solver_device_bytes(const OpoSolver *s);
 void *solver_field(OpoSolver *s, int which);
