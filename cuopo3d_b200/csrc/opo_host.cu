@@ -1177,52 +1177,48 @@ struct TuneEntry {
 std::mutex g_tune_mu;
 std::vector<TuneEntry> g_tune_cache;
 
-template <typename C> int time_pass(OpoSolver *s, int kind, float *ms)
+// Time per launch of `launch` (an enqueue returning an OPO code): 2 warm-up launches,
+// then three rounds of 6, the best round's mean (one slow round -- a clock change, a
+// neighbour's burst -- does not decide a candidate).
+template <typename F> int time_launches(OpoSolver *s, F &&launch, float *ms)
 {
-    const double zh[2] = {0, 0};
-    cudaEvent_t a = nullptr, b = nullptr;
-    OPO_CU(s, cudaEventCreate(&a), "event");
-    OPO_CU(s, cudaEventCreate(&b), "event");
+    constexpr int warm = 2, reps = 6, rounds = 3;
+    cudaEvent_t ev[rounds + 1] = {};
     int rc = OPO_OK;
-    const int warm = 2, reps = 6;
-    for (int r = 0; r < warm + reps && !rc; r++) {
-        if (r == warm) cudaEventRecord(a, s->stream);
-        rc = kind == kT ? enqueue_t<C>(s, false, 2, zh, 0, 7u) : enqueue_axis<C>(s, kind, 0, 7u);
+    for (auto &e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) rc = cuda_fail(s, cudaGetLastError(), "event");
+    for (int r = 0; r < warm && !rc; r++) rc = launch();
+    for (int k = 0; k < rounds && !rc; k++) {
+        cudaEventRecord(ev[k], s->stream);
+        for (int r = 0; r < reps && !rc; r++) rc = launch();
     }
-    cudaEventRecord(b, s->stream);
-    cudaError_t e = cudaEventSynchronize(b);
-    float t = 0;
-    if (!rc && e == cudaSuccess) cudaEventElapsedTime(&t, a, b);
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
+    if (!rc) cudaEventRecord(ev[rounds], s->stream);
+    cudaError_t e = rc ? cudaSuccess : cudaEventSynchronize(ev[rounds]);
+    float best = 0;
+    for (int k = 0; k < rounds && !rc && e == cudaSuccess; k++) {
+        float t = 0;
+        cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+        if (k == 0 || t < best) best = t;
+    }
+    for (auto &x : ev)
+        if (x) cudaEventDestroy(x);
     if (rc) return rc;
     if (e != cudaSuccess) return cuda_fail(s, e, "autotune timing");
-    *ms = t / reps;
+    *ms = best / reps;
     return OPO_OK;
 }
 
-// Mean time of the diffraction operator (plane pass, or x then y pass) over 6 launches.
+template <typename C> int time_pass(OpoSolver *s, int kind, float *ms)
+{
+    const double zh[2] = {0, 0};
+    return time_launches(s, [&] { return kind == kT ? enqueue_t<C>(s, false, 2, zh, 0, 7u) : enqueue_axis<C>(s, kind, 0, 7u); },
+                         ms);
+}
+
+// Time of the diffraction operator (plane pass, or x then y pass), as time_launches.
 template <typename C> int time_diffraction(OpoSolver *s, float *ms)
 {
-    cudaEvent_t a = nullptr, b = nullptr;
-    OPO_CU(s, cudaEventCreate(&a), "event");
-    OPO_CU(s, cudaEventCreate(&b), "event");
-    int rc = OPO_OK;
-    const int warm = 2, reps = 6;
-    for (int r = 0; r < warm + reps && !rc; r++) {
-        if (r == warm) cudaEventRecord(a, s->stream);
-        rc = enqueue_diffraction<C>(s, 0, 7u);
-    }
-    cudaEventRecord(b, s->stream);
-    cudaError_t e = cudaEventSynchronize(b);
-    float t = 0;
-    if (!rc && e == cudaSuccess) cudaEventElapsedTime(&t, a, b);
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-    if (rc) return rc;
-    if (e != cudaSuccess) return cuda_fail(s, e, "autotune timing");
-    *ms = t / reps;
-    return OPO_OK;
+    return time_launches(s, [&] { return enqueue_diffraction<C>(s, 0, 7u); }, ms);
 }
 
 template <typename C> int autotune(OpoSolver *s)
