@@ -159,3 +159,51 @@ def test_line_tpass_batch_equals_standalone(precision):
         for which, a in zip((co.FIELD_AP, co.FIELD_AS, co.FIELD_AI), got):
             assert np.array_equal(a, sim.get_field(which))
         sim.close()
+
+
+@pytest.mark.parametrize("precision", [co.FP32, co.FP64])
+def test_line_tpass_batch_groups_follow_admission_and_retirement(precision):
+    """Under the line setting a batch runs one kernel per line body and one generic
+    kernel, each over its group's share of the descriptors: slots admitted and retired
+    between round trips move instances in and out of the groups (a group emptied, one
+    filled that was empty) without breaking the captured round trip; every surviving slot
+    stays bit for bit its standalone solver."""
+    base = dict(nz=4, LX=300.0, LY=300.0, Lcr=3000.0, FWHM=3.0, t_window=25.0, pump_mode="focused-pulsed",
+                total_rt=4, precision=precision)
+    first = [dict(nx=16, ny=16, nt=256, P=300.0, w0=40.0), dict(nx=16, ny=16, nt=96, P=500.0, w0=35.0),
+             dict(nx=16, ny=32, nt=64, P=200.0, w0=45.0)]
+    later = [dict(nx=32, ny=16, nt=128, P=150.0, w0=60.0, detuning=0.7), dict(nx=16, ny=16, nt=64, P=90.0, w0=30.0)]
+    tun = {"t": dict(threads=128, tile=2048, r1=16 + co.LINE), **AXES}
+    b = co.Batch(precision, 8, 8 << 30, tuning=tun)
+    live = {}
+    for k, inst in enumerate(first):
+        cfg = co.make_config(**{**base, **inst})
+        s = b.add(cfg)
+        b.init_fields(s, cfg, 200 + k, 0.02, idler_copy=True)
+        live[s] = (cfg, 200 + k, 0)
+    b.run_round_trips(1)
+    live = {s: (c, seed, n + 1) for s, (c, seed, n) in live.items()}
+    # retire the 64-sample instance (its group empties), admit a 128-sample one (a group
+    # that was empty) and another 64-sample one
+    gone = [s for s, (c, _, _) in live.items() if c.nt == 64][0]
+    b.remove(gone)
+    del live[gone]
+    for k, inst in enumerate(later):
+        cfg = co.make_config(**{**base, **inst})
+        s = b.add(cfg)
+        b.init_fields(s, cfg, 300 + k, 0.02, idler_copy=True)
+        live[s] = (cfg, 300 + k, 0)
+    b.run_round_trips(2)
+    for s, (cfg, seed, n) in live.items():
+        got = [b.get_field(s, w) for w in (co.FIELD_AP, co.FIELD_AS, co.FIELD_AI)]
+        params, _ = co.derive(cfg)
+        _, w = co.time_freq(cfg.nt, params.t_window)
+        sim = co.Simulation(params, w)
+        sim.set_tuning(tun)
+        sim.set_plane_pass(0)
+        sim.init_fields(cfg, seed, 0.02, idler_copy=True)
+        sim.run_round_trips(n + 2)
+        for which, a in zip((co.FIELD_AP, co.FIELD_AS, co.FIELD_AI), got):
+            assert np.array_equal(a, sim.get_field(which))
+        sim.close()
+    b.close()
