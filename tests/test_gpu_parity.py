@@ -63,10 +63,13 @@ def test_fp64_matches_reference(name):
     assert_close(out, (g.Ap, g.As, g.Ai), FP64_TOL, g.tidx)
 
 
-# Kernel configurations of the headline grid (128 x 128 x 256): the one the benchmark's
-# autotuner chose on a B200 (warp-specialised x and y passes with TMA rings), the
+# Kernel configurations of the headline grid (128 x 128 x 256): the benchmark's (the
+# line-specialised t-pass with warp-specialised x and y passes, as its autotuner picks on
+# a B200), the generic t-pass with warp-specialised x and y passes on TMA rings, the
 # defaults, the classic kernels at the bench's tiles, and the fused plane pass.
 C2_TUNINGS = {
+    "bench_line": {"t": dict(threads=128, tile=1024, r1=4 + co.LINE), "x": dict(threads=160, tile=1024, r1=8),
+                   "y": dict(threads=160, tile=1024, r1=8)},
     "bench_ws": {"t": dict(threads=128, tile=1024, r1=4), "x": dict(threads=160, tile=1024, r1=8),
                  "y": dict(threads=288, tile=2048, r1=8)},
     "default": None,
@@ -97,7 +100,8 @@ def test_c2_headline_fp64_matches_reference(kind):
     elif tun is not None:
         sim.set_tuning(tun)
         sim.set_plane_pass(0)
-        assert all(sim.tuning[k]["threads"] == tun[k]["threads"] for k in "txy")
+        assert all(sim.tuning[k]["threads"] == tun[k]["threads"] and sim.tuning[k]["r1"] == tun[k]["r1"]
+                   for k in "txy")
     s0, i0 = g.initial_fields(co.noise)
     api = co.pump_field(cfg)
     for which, arr in ((co.FIELD_API, api), (co.FIELD_AP, api), (co.FIELD_AS, s0), (co.FIELD_AI, i0)):
