@@ -191,27 +191,36 @@ def c4_instances(n=9, seed=2024):
 @pytest.mark.parametrize("precision,tol", [(co.FP64, 1e-10), (co.FP32, 1e-5)])
 def test_batch_c4_grid_set_vs_oracle(precision, tol):
     """Every grid of the batched form's set in one batch (FP64: the plain form, FP32: the
-    precision form) against the FP64 oracle on the same inputs, two round trips."""
+    precision form) against the FP64 oracle on the same inputs, two round trips; once
+    with the generic t-pass and once with the line-specialised one (one batched kernel
+    per line body: the time axes 64, 128 and 256 of the set), the setting the batch tuner
+    picks for the C4 mix."""
     insts = c4_instances()
-    tuning = TUNING if precision == co.FP64 else {"t": dict(threads=128, tile=2048, r1=8),
-                                                  "x": dict(threads=128, tile=2048, r1=8),
-                                                  "y": dict(threads=128, tile=2048, r1=16)}
-    b = co.Batch(precision, len(insts), 16 << 30, tuning=tuning)
-    slots = []
+    generic = TUNING if precision == co.FP64 else {"t": dict(threads=128, tile=2048, r1=8),
+                                                   "x": dict(threads=128, tile=2048, r1=8),
+                                                   "y": dict(threads=128, tile=2048, r1=16)}
+    line_t = dict(threads=128, tile=512, r1=4 + co.LINE) if precision == co.FP64 else \
+        dict(threads=128, tile=2048, r1=16 + co.LINE)
+    refs = []
     for k, kw in enumerate(insts):
-        cfg = co.make_config(precision=precision, **kw)
-        s = b.add(cfg)
-        b.init_fields(s, cfg, 300 + k, 0.01)
-        slots.append(s)
-    b.run_round_trips(2)
-    for k, kw in enumerate(insts):
-        got = [b.get_field(slots[k], w) for w in (co.FIELD_AP, co.FIELD_AS, co.FIELD_AI)]
         st = po.Setup(po.make_phys(**kw))
         api = st.api_complex()
         s0 = co.noise(300 + k, 0.01, api.size).reshape(api.shape)
-        ref = po.round_trips(st, api, api, s0, np.zeros_like(s0), 2)
-        for name, a, c in zip(("Ap", "As", "Ai"), got, ref):
-            assert rel_l2(a, c) < tol, (kw["nx"], kw["nt"], name, rel_l2(a, c))
+        refs.append(po.round_trips(st, api, api, s0, np.zeros_like(s0), 2))
+    for tuning in (generic, {**generic, "t": line_t}):
+        b = co.Batch(precision, len(insts), 16 << 30, tuning=tuning)
+        slots = []
+        for k, kw in enumerate(insts):
+            cfg = co.make_config(precision=precision, **kw)
+            s = b.add(cfg)
+            b.init_fields(s, cfg, 300 + k, 0.01)
+            slots.append(s)
+        b.run_round_trips(2)
+        for k, kw in enumerate(insts):
+            got = [b.get_field(slots[k], w) for w in (co.FIELD_AP, co.FIELD_AS, co.FIELD_AI)]
+            for name, a, c in zip(("Ap", "As", "Ai"), got, refs[k]):
+                assert rel_l2(a, c) < tol, (tuning["t"], kw["nx"], kw["nt"], name, rel_l2(a, c))
+        b.close()
 
 
 @pytest.mark.parametrize("mode", sorted(co.PUMP_MODES))
